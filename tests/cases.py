@@ -1,0 +1,176 @@
+"""Seeded survey cases shared by the golden-fixture script and the tests.
+
+Each case is a dict: ``inpa`` (the reference's input-parameter dict),
+``src_loc`` / ``rec_loc`` (metres, columns x then z), ``fdom``, ``src_type``,
+``components``, ``chpr``, ``n_well_rec``, ``param`` ('dv' or 'lmd') and two
+models ``model_obs`` / ``model_est`` of (nz, nx) float32 arrays.
+
+``c1`` is the 100 x 100, 4-shot, 500-step survey with a circular anomaly; the
+``tiny_*`` cases each exercise one corner of the reference's behaviour
+(8th order, sub-stepped time, reverse-time reconstruction, crosswell and
+two-well geometries, receiver spacing, directional sources, damping layouts).
+"""
+import numpy as np
+
+
+def _t_for(nt, dt):
+    # the reference takes nt = int(1 + t // dt); half a step of margin keeps
+    # the float floor from dropping the last step
+    return (nt - 1) * dt + dt / 2
+
+
+def circle_model(nz, nx, vp, vs, rho, centre, radius, pert):
+    """Homogeneous model plus a disc (cells with (z-zc)^2 + (x-xc)^2 < r^2)
+    scaled by (1 + pert)."""
+    zz, xx = np.meshgrid(np.arange(nz), np.arange(nx), indexing="ij")
+    disc = (zz - centre[0]) ** 2 + (xx - centre[1]) ** 2 < radius ** 2
+    m = {"vp": np.full((nz, nx), vp, np.float32), "vs": np.full((nz, nx), vs, np.float32),
+         "rho": np.full((nz, nx), rho, np.float32)}
+    for k in m:
+        m[k][disc] *= np.float32(1 + pert)
+    return m
+
+
+def layered_model(nz, nx, seed, vp_lo=1500.0, vp_hi=2000.0, ratio=1.8):
+    """Smooth random layered model: vp rises with depth plus a seeded bump."""
+    rng = np.random.default_rng(seed)
+    z = np.linspace(0, 1, nz)[:, None]
+    x = np.linspace(0, 1, nx)[None, :]
+    vp = vp_lo + (vp_hi - vp_lo) * z + 0 * x
+    cz, cx, r = rng.uniform(0.3, 0.7), rng.uniform(0.3, 0.7), rng.uniform(0.1, 0.2)
+    vp = vp * (1 + 0.05 * np.exp(-((z - cz) ** 2 + (x - cx) ** 2) / r ** 2))
+    vp = vp.astype(np.float32)
+    vs = (vp / ratio).astype(np.float32)
+    rho = (310 * vp ** 0.25).astype(np.float32)
+    return {"vp": vp, "vs": vs, "rho": rho}
+
+
+def perturbed(model, seed, amp=0.05):
+    rng = np.random.default_rng(seed)
+    nz, nx = model["vp"].shape
+    bump = np.zeros((nz, nx), np.float32)
+    cz, cx = rng.integers(nz // 3, 2 * nz // 3), rng.integers(nx // 3, 2 * nx // 3)
+    zz, xx = np.meshgrid(np.arange(nz), np.arange(nx), indexing="ij")
+    bump[(zz - cz) ** 2 + (xx - cx) ** 2 < (min(nz, nx) // 5) ** 2] = amp
+    return {k: (v * (1 + bump)).astype(np.float32) for k, v in model.items()}
+
+
+def c1():
+    """100 x 100 cells, dh = 1 m, 20-cell absorbing layer; vp = 2500, vs =
+    vp / 1.73, rho = 2000 plus a radius-15 disc at +10 % for the observed
+    data; four explosive 60 Hz Ricker shots and 100 receivers at z = 2 cells;
+    dt = 0.2 ms, nt = 500; vx and vz recorded; every step checkpointed."""
+    nz = nx = 100
+    dh, dt = 1.0, 0.0002
+    inpa = {"dt": dt, "t": _t_for(500, dt), "dh": dh, "npml": 20, "pmlR": 1e-5, "pml_dir": 2, "sdo": 4,
+            "rec_dis": dh, "acq_type": 1}
+    ns = 4
+    src_loc = np.zeros((ns, 2), np.float32)
+    src_loc[:, 0] = ((np.arange(ns) + 0.5) * nx / ns).astype(np.int32) * dh
+    src_loc[:, 1] = 2 * dh
+    rec_loc = np.zeros((nx, 2), np.float32)
+    rec_loc[:, 0] = np.arange(nx) * dh
+    rec_loc[:, 1] = 2 * dh
+    vp = 2500.0
+    bg = circle_model(nz, nx, vp, vp / 1.73, 2000.0, (50, 50), 15, 0.0)
+    obs = circle_model(nz, nx, vp, vp / 1.73, 2000.0, (50, 50), 15, 0.10)
+    return dict(name="c1", inpa=inpa, src_loc=src_loc, rec_loc=rec_loc, fdom=60.0, src_type=0, components=2,
+                chpr=100, n_well_rec=0, param="dv", model_obs=obs, model_est=bg)
+
+
+def _surface(nz, nx, dh, ns, rec_depth, src_depth, rec_step=1, rec_first=0, rec_last=None, src_x=None):
+    rec_last = nx if rec_last is None else rec_last
+    xs = np.arange(rec_first, rec_last, rec_step)
+    rec_loc = np.stack([xs * dh, np.full(xs.size, rec_depth * dh)], 1).astype(np.float32)
+    src_loc = np.zeros((ns, 2), np.float32)
+    src_loc[:, 0] = (np.linspace(4, nx - 5, ns).astype(np.int32) if src_x is None else np.asarray(src_x)) * dh
+    src_loc[:, 1] = src_depth * dh
+    return src_loc, rec_loc
+
+
+def tiny_s8():
+    """8th-order stencil, all five components, energy-balanced 'lmd' gradient."""
+    nz, nx, dh, dt = 30, 40, 2.0, 0.0004
+    inpa = {"dt": dt, "t": _t_for(150, dt), "dh": dh, "npml": 6, "pmlR": 1e-5, "pml_dir": 2, "sdo": 8,
+            "rec_dis": dh, "acq_type": 1, "energy_balancing": True}
+    src_loc, rec_loc = _surface(nz, nx, dh, 2, rec_depth=3, src_depth=4, src_x=[10, 28])
+    est = layered_model(nz, nx, 1)
+    return dict(name="tiny_s8", inpa=inpa, src_loc=src_loc, rec_loc=rec_loc, fdom=80.0, src_type=0,
+                components=4, chpr=100, n_well_rec=0, param="lmd", model_obs=perturbed(est, 2), model_est=est)
+
+
+def tiny_dtscale():
+    """dt = 1.1 ms: the propagator splits each sample into two steps."""
+    nz, nx, dh, dt = 32, 36, 2.0, 0.0011
+    inpa = {"dt": dt, "t": 0.13, "dh": dh, "npml": 5, "pmlR": 1e-5, "pml_dir": 2, "rec_dis": dh,
+            "acq_type": 1}
+    src_loc, rec_loc = _surface(nz, nx, dh, 2, rec_depth=2, src_depth=3, rec_first=1, rec_last=nx - 1)
+    est = layered_model(nz, nx, 3, 1400.0, 1900.0)
+    return dict(name="tiny_dtscale", inpa=inpa, src_loc=src_loc, rec_loc=rec_loc, fdom=40.0, src_type=0,
+                components=0, chpr=100, n_well_rec=0, param="dv", model_obs=perturbed(est, 4), model_est=est)
+
+
+def tiny_chpr():
+    """10 % checkpoints: the backward pass reconstructs the rest in reverse time."""
+    nz, nx, dh, dt = 28, 34, 2.0, 0.0004
+    inpa = {"dt": dt, "t": _t_for(140, dt), "dh": dh, "npml": 5, "pmlR": 1e-5, "pml_dir": 3, "rec_dis": dh,
+            "acq_type": 1}
+    src_loc, rec_loc = _surface(nz, nx, dh, 3, rec_depth=2, src_depth=2)
+    est = layered_model(nz, nx, 5)
+    return dict(name="tiny_chpr", inpa=inpa, src_loc=src_loc, rec_loc=rec_loc, fdom=70.0, src_type=0,
+                components=3, chpr=10, n_well_rec=0, param="dv", model_obs=perturbed(est, 6), model_est=est)
+
+
+def tiny_crosswell():
+    """Crosswell geometry (receivers down a column), no x damping, chpr = 0."""
+    nz, nx, dh, dt = 36, 30, 2.0, 0.0004
+    inpa = {"dt": dt, "t": _t_for(130, dt), "dh": dh, "npml": 5, "pmlR": 1e-5, "pml_dir": 0, "rec_dis": dh,
+            "acq_type": 0, "sdo": 4}
+    zs = np.arange(3, nz - 3)
+    rec_loc = np.stack([np.full(zs.size, (nx - 4) * dh), zs * dh], 1).astype(np.float32)
+    src_loc = np.array([[4 * dh, 10 * dh], [4 * dh, 24 * dh]], np.float32)
+    est = layered_model(nz, nx, 7)
+    return dict(name="tiny_crosswell", inpa=inpa, src_loc=src_loc, rec_loc=rec_loc, fdom=70.0, src_type=0,
+                components=1, chpr=0, n_well_rec=0, param="dv", model_obs=perturbed(est, 8), model_est=est)
+
+
+def tiny_dxr():
+    """Receivers every second cell up to the right edge, no z damping, a
+    directional (vx) source."""
+    nz, nx, dh, dt = 30, 38, 2.0, 0.0004
+    inpa = {"dt": dt, "t": _t_for(140, dt), "dh": dh, "npml": 4, "pmlR": 1e-5, "pml_dir": 1,
+            "rec_dis": 2 * dh, "acq_type": 1}
+    src_loc, rec_loc = _surface(nz, nx, dh, 2, rec_depth=3, src_depth=5, rec_step=2, rec_first=1)
+    est = layered_model(nz, nx, 9)
+    return dict(name="tiny_dxr", inpa=inpa, src_loc=src_loc, rec_loc=rec_loc, fdom=70.0, src_type=1,
+                components=2, chpr=100, n_well_rec=0, param="dv", model_obs=perturbed(est, 10), model_est=est)
+
+
+def tiny_both():
+    """Surface line plus two wells (acq_type 2), all components."""
+    nz, nx, dh, dt = 30, 34, 2.0, 0.0004
+    inpa = {"dt": dt, "t": _t_for(120, dt), "dh": dh, "npml": 5, "pmlR": 1e-5, "pml_dir": 2, "rec_dis": dh,
+            "acq_type": 2, "sdo": 4}
+    # layout of acquisition.acq_parameters(acq_type=2): left well, surface line, right well
+    zs = np.arange(4, nz - 4)
+    left = np.stack([np.full(zs.size, 3 * dh), zs * dh], 1)
+    xs = np.arange(4, nx - 4)
+    surf = np.stack([xs * dh, np.full(xs.size, 3 * dh)], 1)
+    right = np.stack([np.full(zs.size, (nx - 4) * dh), zs * dh], 1)
+    rec_loc = np.vstack([left, surf, right]).astype(np.float32)
+    src_loc = np.array([[12 * dh, 4 * dh], [22 * dh, 4 * dh]], np.float32)
+    est = layered_model(nz, nx, 11)
+    return dict(name="tiny_both", inpa=inpa, src_loc=src_loc, rec_loc=rec_loc, fdom=70.0, src_type=0,
+                components=4, chpr=100, n_well_rec=int(zs.size), param="dv", model_obs=perturbed(est, 12),
+                model_est=est)
+
+
+TINY = [tiny_s8, tiny_dtscale, tiny_chpr, tiny_crosswell, tiny_dxr, tiny_both]
+ALL = [c1] + TINY
+
+
+def by_name(name):
+    for f in ALL:
+        if f.__name__ == name:
+            return f()
+    raise KeyError(name)

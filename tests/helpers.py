@@ -1,0 +1,26 @@
+"""Shared helpers for the tests: build inputs of a case the way a PyFWI user
+would, and run the oracle on them."""
+import numpy as np
+
+import cases
+
+
+def oracle_run(case, precision="fp32", d_obs=None, gradient=True):
+    """Run the CPU oracle on a case: (d_obs, d_est, grad, propagator)."""
+    import oracle as O
+    inpa = case["inpa"]
+    src = O.Ricker(case["src_loc"], inpa["dh"], inpa["dt"], case["src_type"])
+    src.Ricker(case["fdom"])
+    kw = dict(components=case["components"], n_well_rec=case["n_well_rec"], precision=precision)
+    shape = case["model_est"]["vp"].shape
+    if d_obs is None:
+        Wo = O.OracleWavePropagator(inpa, src, case["rec_loc"], shape, chpr=0, **kw)
+        d_obs = Wo.forward_modeling({k: v.copy() for k, v in case["model_obs"].items()})
+    W = O.OracleWavePropagator(inpa, src, case["rec_loc"], shape, chpr=case["chpr"], **kw)
+    d_est = W.forward_modeling({k: v.copy() for k, v in case["model_est"].items()})
+    grad = None
+    if gradient:
+        pe, po = O.prepare_residual(d_est, 1), O.prepare_residual(d_obs, 1)
+        res = {k: (pe[k] - po[k]).astype(W.real) for k in O.FIELDS}
+        grad = W.gradient(res, parameterization=case["param"])
+    return d_obs, d_est, grad, W
