@@ -1,0 +1,170 @@
+/*
+ * pyfwi_b200 -- C ABI of the B200 elastic propagator and adjoint gradient.
+ *
+ * This is the native boundary under the Python drop-in for PyFWI's hot path
+ * (PyFWI src/PyFWI/wave_propagation.py: WavePropagator.forward_modeling and
+ * WavePropagator.gradient).  In the reference that boundary is a set of
+ * OpenCL kernels launched through pyopencl once per time step and shot
+ * (wave_propagation.py:625-856); here one call runs every time step of every
+ * shot on the device.
+ *
+ * Conventions
+ *  - Every function returns an int status: PYFWI_OK (0) or a negative code;
+ *    pyfwi_last_error() gives the message of the calling thread's last error.
+ *  - All array arguments except those marked "host" are device pointers.
+ *    The caller owns all device memory: inputs, outputs and one workspace of
+ *    pyfwi_workspace_size() bytes (256-byte aligned).  No call allocates or
+ *    frees device memory.
+ *  - `stream` is a cudaStream_t passed as void*.  Calls only enqueue work on
+ *    it (plus small host-to-device copies of constants on the same stream);
+ *    they do not synchronise except where stated.
+ *  - A plan is not thread-safe: use one plan per host thread/stream.
+ *  - Grid coordinates: the padded grid has nz + 2*npml rows (z) and
+ *    nx + 2*npml columns (x); cell (i, j) is row i, column j.
+ */
+#ifndef PYFWI_B200_H
+#define PYFWI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PYFWI_ABI_VERSION 1
+
+enum pyfwi_status {
+    PYFWI_OK = 0,
+    PYFWI_E_INVALID = -1,   /* bad argument or geometry */
+    PYFWI_E_WORKSPACE = -2, /* workspace missing or smaller than required */
+    PYFWI_E_CUDA = -3,      /* a CUDA runtime call failed */
+    PYFWI_E_TIMEOUT = -4,   /* a bounded device-side wait gave up */
+    PYFWI_E_STATE = -5      /* call out of order (e.g. gradient before forward) */
+};
+
+enum pyfwi_checkpoint {
+    /* Exact: the adjoint sees the forward state of every step, stored or
+     * recomputed from restart states; identical to the reference with
+     * chpr = 100 (wave_propagation.py:95-100, 710-727, 761-779). */
+    PYFWI_CKPT_EXACT = 0,
+    /* The reference's chpr < 100 scheme: states stored at the listed steps,
+     * the rest rebuilt by reverse-time steps (wave_propagation.py:761-812). */
+    PYFWI_CKPT_REVERSE = 1
+};
+
+enum pyfwi_snapshot { PYFWI_SNAP_FP32 = 0, PYFWI_SNAP_BF16 = 1 };
+
+enum pyfwi_parameterization { PYFWI_PARAM_LMD = 0, PYFWI_PARAM_DV = 1 };
+
+/* One straight line of receivers.  Receiver k (0 <= k < count) sits at cell
+ * (row0 + k*drow, col0 + k*dcol) and fills trace slot slot0 + k.  The three
+ * receiver groups of the reference kernels (elastic_surface.cl:30-39,
+ * elastic_crosswell.cl:95-102, elastic.cl:65-96) are each one line. */
+typedef struct pyfwi_rec_line {
+    int32_t row0, col0;
+    int32_t drow, dcol;
+    int32_t count;
+    int32_t slot0;
+    int32_t vz_from_vx; /* 1: the vz trace records vx (elastic_crosswell.cl:98) */
+} pyfwi_rec_line;
+
+/* Survey geometry.  Mirrors the compile-time macros the reference builds per
+ * WavePropagator (wave_propagation.py:423-490) plus the per-shot source cells
+ * (wave_propagation.py:86-87). */
+typedef struct pyfwi_geometry {
+    int32_t nz, nx;         /* model grid, without the absorbing layer */
+    int32_t npml;           /* absorbing-layer width in cells */
+    int32_t half_order;     /* sdo: 2 (4th-order stencil) or 4 (8th) */
+    int32_t nt;             /* internal time steps */
+    int32_t nt_ext;         /* trace samples */
+    int32_t dt_scale;       /* internal steps per trace sample */
+    float dt;               /* internal step (s) */
+    float dh;               /* cell size (m) */
+    float c[4];             /* stencil coefficients c1..c4 */
+    int32_t ns;             /* shots */
+    int32_t nr;             /* trace slots per shot */
+    int32_t n_lines;        /* receiver lines, 1..3 */
+    pyfwi_rec_line lines[3];
+    /* Gradient window in model-grid cells, [row0,row1) x [col0,col1): the
+     * region gradient_reading keeps (wave_propagation.py:303-318). */
+    int32_t mask_row0, mask_row1, mask_col0, mask_col1;
+} pyfwi_geometry;
+
+/* Run options. */
+typedef struct pyfwi_options {
+    int32_t checkpoint;     /* enum pyfwi_checkpoint */
+    int32_t segment;        /* exact mode: steps per recompute segment; 0 = all steps */
+    int32_t snapshot;       /* exact mode: enum pyfwi_snapshot for stored states */
+    int32_t shot_batch;     /* shots propagated together; 0 = all */
+    int32_t energy;         /* 1: also accumulate the energy terms (energy_balancing) */
+    int32_t nchp;           /* reverse mode: number of checkpoint steps */
+    const int32_t *chp;     /* host; reverse mode: the checkpoint steps (copied) */
+    int32_t tile;           /* kernel tile variant, 0 = default (see pyfwi_tile_count) */
+    int32_t graph;          /* 1: replay time loops as CUDA graphs */
+} pyfwi_options;
+
+typedef struct pyfwi_plan pyfwi_plan;
+
+/* Build a plan.  srcx, srcz: host arrays of ns padded-grid source cells
+ * (replaces WavePreparation.__init__, wave_propagation.py:18-246, on the
+ * native side).  Allocates host memory only. */
+int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int32_t *srcz,
+                      const pyfwi_options *opt, pyfwi_plan **plan);
+int pyfwi_plan_destroy(pyfwi_plan *plan);
+
+/* Bytes of device workspace the plan needs. */
+int pyfwi_workspace_size(const pyfwi_plan *plan, size_t *bytes);
+
+/* Load a model into the workspace: pad by edge replication, form
+ * mu = rho*vs^2, lam = rho*vp^2 - 2*mu, buoyancy 1/rho, and scale the
+ * damping profiles by max(vp).  Replaces expand_model (fwi_tools.py:776-811),
+ * pml_preparation (wave_propagation.py:400-407) and elastic_buffers
+ * (wave_propagation.py:570-591).
+ *   vp, vs, rho   [nz][nx] float32
+ *   damp_x        [nx + 2*npml] damping profile per column (before the vp_max factor)
+ *   damp_z        [nz + 2*npml] damping profile per row */
+int pyfwi_set_model(pyfwi_plan *plan, void *workspace, size_t workspace_bytes, const float *vp,
+                    const float *vs, const float *rho, const float *damp_x, const float *damp_z, void *stream);
+
+/* Forward modelling of every shot.  Replaces forward_propagator and its
+ * per-step loop (wave_propagation.py:625-733).
+ *   src_vals  host [n_src][4]: (vx, vz, taux, tauz) amplitudes added at the
+ *             source cell on injection k; injections past n_src add zero
+ *   traces    [5][nt_ext][ns*nr]: vx, vz, taux, tauz, tauxz; column s*nr + r
+ *             is receiver slot r of shot s (the reference's '2d' layout) */
+int pyfwi_forward(pyfwi_plan *plan, void *workspace, size_t workspace_bytes, const float *src_vals,
+                  int32_t n_src, float *traces, void *stream);
+
+/* Adjoint-state gradient for the last forward call's model and sources.
+ * Replaces __adjoint_modelling_per_source, __kernel_gradient and
+ * gradient_reading + grad_lmd_to_vd (wave_propagation.py:735-856, 279-331,
+ * grad_switcher.py:331-383).
+ *   residual  5 device pointers (vx, vz, taux, tauz, tauxz), each
+ *             [nt_ext][ns*nr]; NULL means an all-zero component
+ *   grad      [3][nz][nx]: (lam, mu, rho) or (vp, vs, rho) per `parameterization`
+ *   raw       optional [6][nz+2npml][nx+2npml]: the accumulators
+ *             (Gmu, Glam, Grho, and the three energy terms) before masking */
+int pyfwi_gradient(pyfwi_plan *plan, void *workspace, size_t workspace_bytes, const float *const *residual,
+                   int32_t parameterization, float *grad, float *raw, void *stream);
+
+/* L2 misfit and residual (CostFunction.l2, fwi_tools.py:1402-1422):
+ * res = est - obs (float32), *misfit += 0.5 * sum(res^2) (float64 sum on device). */
+int pyfwi_l2_residual(const float *est, const float *obs, float *res, int64_t n, double *misfit, void *stream);
+
+/* Trace section (acquisition.py:313-333): out = (a + b) / 2 elementwise. */
+int pyfwi_mean2(const float *a, const float *b, float *out, int64_t n, void *stream);
+
+/* Number of kernel tile variants the autotuner may choose between. */
+int pyfwi_tile_count(int32_t half_order);
+
+/* Kernel launches this plan issued since creation (for launch accounting). */
+int pyfwi_launch_count(const pyfwi_plan *plan, int64_t *count);
+
+const char *pyfwi_last_error(void);
+int pyfwi_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PYFWI_B200_H */

@@ -156,7 +156,8 @@ def build_for(name, **geom):
             src = f.read()
         so, kernels = compile_program(macro + src)
         entry[prog] = {"so": os.path.relpath(so, HERE), "kernels": kernels}
-    entry["geom"] = {k: (list(v) if isinstance(v, tuple) else v) for k, v in geom.items()}
+    entry["geom"] = {k: ([float(x) for x in v] if isinstance(v, tuple) else (v.item() if hasattr(v, "item") else v))
+                     for k, v in geom.items()}
     man = load_manifest()
     man[name] = entry
     with open(os.path.join(REF_OUT, "manifest.json"), "w") as f:

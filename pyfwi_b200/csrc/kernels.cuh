@@ -1,0 +1,849 @@
+// Device code of the B200 elastic propagator.
+//
+// One kernel launch advances every shot of a batch by one time step.  Each
+// CTA owns a TZ x TX tile of one shot (blockIdx.z) and fuses what the
+// reference does in four to six full-grid OpenCL launches per step
+// (PyFWI src/PyFWI/elastic.cl:155-308, 372-526, elastic_surface.cl:7-71):
+//   forward  : source add -> velocity update on the tile plus an R-cell ring
+//              -> stress update on the tile, reading the new velocities from
+//              shared memory; receiver traces are recorded from the input
+//              state (before the source add);
+//   reverse  : the same with stress first (reverse-time reconstruction);
+//   adjoint  : residual injection -> adjoint stress on tile + ring ->
+//              adjoint velocity on the tile -> zero-lag imaging accumulation.
+// Fields are FP32 planes in a padded layout (see Grid) whose frame is zero,
+// so stencils never branch on the grid edge.  Arithmetic is FP32 with FMA.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pyfwi {
+
+// Padded plane layout: grid cell (i, j) lives at (i + ZO) * pitch + (j + XO).
+// The frame (ZO rows above/below, >= XO columns left/right) stays zero.
+constexpr int XO = 8;
+constexpr int ZO = 8;
+constexpr int TX = 64;         // tile width in cells (all variants)
+constexpr int NTHREADS = 256;  // threads per CTA (all variants)
+
+enum Field { VX = 0, VZ = 1, TXX = 2, TZZ = 3, TXZ = 4 };
+
+struct Grid {
+    int tnz, tnx;    // padded grid (model + absorbing layer)
+    int pitch;       // floats per allocated row, multiple of 32
+    int rows;        // allocated rows, tnz + 2 * ZO
+    long long plane; // pitch * rows
+};
+
+struct Coef {
+    float cx[4];  // c_k / dh (x derivatives)
+    float cz[4];  // c_k / dh (z derivatives)
+    float dt;
+};
+
+struct Lines {
+    int n;
+    int row0[3], col0[3], drow[3], dcol[3], count[3], slot0[3], vzx[3];
+};
+
+__device__ __forceinline__ long long cell_off(const Grid &g, int i, int j)
+{
+    return (long long)(i + ZO) * g.pitch + (j + XO);
+}
+
+// One float4 of a padded plane; zero outside the allocation.  gj must be a
+// multiple of 4 (rows start 128-byte aligned and XO is a multiple of 4).
+__device__ __forceinline__ float4 ld4(const float *plane, const Grid &g, int gi, int gj)
+{
+    int ar = gi + ZO, ac = gj + XO;
+    if (ar < 0 || ar >= g.rows || ac < 0 || ac + 3 >= g.pitch) return make_float4(0.f, 0.f, 0.f, 0.f);
+    return __ldg(reinterpret_cast<const float4 *>(plane + (long long)ar * g.pitch + ac));
+}
+
+__device__ __forceinline__ void st4s(float *s, float4 v) { *reinterpret_cast<float4 *>(s) = v; }
+
+// ---- staggered one-sided differences on a shared-memory array -------------
+// fwd: c1(f[+1]-f[0]) + c2(f[+2]-f[-1]) [+ c3(f[+3]-f[-2]) + c4(f[+4]-f[-3])]
+// bwd: c1(f[0]-f[-1]) + c2(f[+1]-f[-2]) [+ c3(f[+2]-f[-3]) + c4(f[+3]-f[-4])]
+// with c_k already divided by dh; s is the element stride of the direction.
+template <int R>
+__device__ __forceinline__ float dfwd(const float *f, int i, int s, const float *c)
+{
+    float r = c[0] * (f[i + s] - f[i]);
+    r = fmaf(c[1], f[i + 2 * s] - f[i - s], r);
+    if (R == 4) {
+        r = fmaf(c[2], f[i + 3 * s] - f[i - 2 * s], r);
+        r = fmaf(c[3], f[i + 4 * s] - f[i - 3 * s], r);
+    }
+    return r;
+}
+
+template <int R>
+__device__ __forceinline__ float dbwd(const float *f, int i, int s, const float *c)
+{
+    float r = c[0] * (f[i] - f[i - s]);
+    r = fmaf(c[1], f[i + s] - f[i - 2 * s], r);
+    if (R == 4) {
+        r = fmaf(c[2], f[i + 2 * s] - f[i - 3 * s], r);
+        r = fmaf(c[3], f[i + 3 * s] - f[i - 4 * s], r);
+    }
+    return r;
+}
+
+// Differences of a pointwise product a*b (adjoint kernels, elastic.cl:385-463).
+template <int R>
+__device__ __forceinline__ float dfwd_p(const float *a, const float *b, int i, int s, const float *c)
+{
+#define P_(k) (a[(k)] * b[(k)])
+    float r = c[0] * (P_(i + s) - P_(i));
+    r = fmaf(c[1], P_(i + 2 * s) - P_(i - s), r);
+    if (R == 4) {
+        r = fmaf(c[2], P_(i + 3 * s) - P_(i - 2 * s), r);
+        r = fmaf(c[3], P_(i + 4 * s) - P_(i - 3 * s), r);
+    }
+    return r;
+}
+
+template <int R>
+__device__ __forceinline__ float dbwd_p(const float *a, const float *b, int i, int s, const float *c)
+{
+    float r = c[0] * (P_(i) - P_(i - s));
+    r = fmaf(c[1], P_(i + s) - P_(i - 2 * s), r);
+    if (R == 4) {
+        r = fmaf(c[2], P_(i + 2 * s) - P_(i - 3 * s), r);
+        r = fmaf(c[3], P_(i + 3 * s) - P_(i - 4 * s), r);
+    }
+    return r;
+#undef P_
+}
+
+// Differences of (lam + 2 mu) * A.
+template <int R>
+__device__ __forceinline__ float dfwd_l2m(const float *lam, const float *mu, const float *A, int i, int s,
+                                          const float *c)
+{
+#define L_(k) ((lam[(k)] + 2.f * mu[(k)]) * A[(k)])
+    float r = c[0] * (L_(i + s) - L_(i));
+    r = fmaf(c[1], L_(i + 2 * s) - L_(i - s), r);
+    if (R == 4) {
+        r = fmaf(c[2], L_(i + 3 * s) - L_(i - 2 * s), r);
+        r = fmaf(c[3], L_(i + 4 * s) - L_(i - 3 * s), r);
+    }
+    return r;
+}
+
+template <int R>
+__device__ __forceinline__ float dbwd_l2m(const float *lam, const float *mu, const float *A, int i, int s,
+                                          const float *c)
+{
+    float r = c[0] * (L_(i) - L_(i - s));
+    r = fmaf(c[1], L_(i + s) - L_(i - 2 * s), r);
+    if (R == 4) {
+        r = fmaf(c[2], L_(i + 2 * s) - L_(i - 3 * s), r);
+        r = fmaf(c[3], L_(i + 3 * s) - L_(i - 4 * s), r);
+    }
+    return r;
+#undef L_
+}
+
+// Same differences read straight from a global plane (imaging stencils).
+template <int R>
+__device__ __forceinline__ float gfwd(const float *f, long long i, long long s, const float *c)
+{
+    float r = c[0] * (__ldg(f + i + s) - __ldg(f + i));
+    r = fmaf(c[1], __ldg(f + i + 2 * s) - __ldg(f + i - s), r);
+    if (R == 4) {
+        r = fmaf(c[2], __ldg(f + i + 3 * s) - __ldg(f + i - 2 * s), r);
+        r = fmaf(c[3], __ldg(f + i + 4 * s) - __ldg(f + i - 3 * s), r);
+    }
+    return r;
+}
+
+template <int R>
+__device__ __forceinline__ float gbwd(const float *f, long long i, long long s, const float *c)
+{
+    float r = c[0] * (__ldg(f + i) - __ldg(f + i - s));
+    r = fmaf(c[1], __ldg(f + i + s) - __ldg(f + i - 2 * s), r);
+    if (R == 4) {
+        r = fmaf(c[2], __ldg(f + i + 2 * s) - __ldg(f + i - 3 * s), r);
+        r = fmaf(c[3], __ldg(f + i + 3 * s) - __ldg(f + i - 4 * s), r);
+    }
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// kernel arguments
+// ---------------------------------------------------------------------------
+struct StepArgs {
+    Grid g;
+    Coef k;
+    const float *in;       // input state of slot 0: [5][plane]
+    float *out;            // output state of slot 0
+    long long in_stride;   // elements between the states of consecutive slots
+    long long out_stride;
+    const float *mat;      // [4][plane]: lam, mu, buoyancy, rho
+    const float *dampx;    // [pitch] damping per allocated column (x 1/s)
+    const float *dampz;    // [rows] damping per allocated row
+    int shot0;             // shot of slot 0
+    const int *srcx;       // [ns] padded-grid source column per shot
+    const int *srcz;       // [ns] source row per shot
+    float4 src;            // (vx, vz, taux, tauz) added this step
+    int add_src;
+    int rec_row;           // trace row recorded this step, -1 for none
+    float *traces;         // [5][nt_ext][ns*nr]
+    long long trace_plane; // nt_ext * ns * nr
+    int nr;
+    int ns;
+    Lines lines;
+};
+
+struct AdjArgs {
+    Grid g;
+    Coef k;
+    const float *in;       // adjoint state in, slot 0
+    float *out;            // adjoint state out
+    long long in_stride, out_stride;
+    const float *fwd;      // forward state S_{t+1}, slot 0 (FP32)
+    const __nv_bfloat16 *fwd16;  // same, BF16 snapshot (used when fwd == nullptr)
+    long long fwd_stride;
+    float *gacc;           // [slot][3 or 6][plane] accumulators
+    long long gacc_stride;
+    const float *mat;
+    const float *dampx, *dampz;
+    int npml;
+    int shot0;
+    int inj_row;           // residual row injected this step, -1 for none
+    const float *res[5];   // [nt_ext][ns*nr] residual components (nullable)
+    int nr, ns;
+    Lines lines;
+};
+
+__device__ __forceinline__ bool in_domain(const Grid &g, int R, int i, int j)
+{
+    return i >= R && i <= g.tnz - R && j >= R && j <= g.tnx - R;
+}
+
+// Record the five fields of `st` at cell (i, j) into every trace slot whose
+// receiver sits there.
+__device__ __forceinline__ void record_cell(const StepArgs &a, const float *st, int shot, int i, int j)
+{
+    const Lines &L = a.lines;
+    for (int l = 0; l < L.n; ++l) {
+        int k;
+        if (L.drow[l] == 0) {
+            int d = j - L.col0[l];
+            if (i != L.row0[l] || d < 0 || d % L.dcol[l]) continue;
+            k = d / L.dcol[l];
+        } else {
+            int d = i - L.row0[l];
+            if (j != L.col0[l] || d < 0 || d % L.drow[l]) continue;
+            k = d / L.drow[l];
+        }
+        if (k >= L.count[l]) continue;
+        long long o = (long long)a.rec_row * a.ns * a.nr + (long long)shot * a.nr + L.slot0[l] + k;
+        long long c = cell_off(a.g, i, j);
+        float vx = st[VX * a.g.plane + c];
+        a.traces[0 * a.trace_plane + o] = vx;
+        a.traces[1 * a.trace_plane + o] = L.vzx[l] ? vx : st[VZ * a.g.plane + c];
+        a.traces[2 * a.trace_plane + o] = st[TXX * a.g.plane + c];
+        a.traces[3 * a.trace_plane + o] = st[TZZ * a.g.plane + c];
+        a.traces[4 * a.trace_plane + o] = st[TXZ * a.g.plane + c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// forward step: velocities then stresses (elastic.cl:155-308, coeff = +1)
+// ---------------------------------------------------------------------------
+template <int R, int TZ>
+struct FwdShape {
+    static constexpr int W = TX + 4 * R;   // shared row width
+    static constexpr int HT = TZ + 4 * R;  // stress rows (tile + 2R halo)
+    static constexpr int HV = TZ + 2 * R;  // velocity rows (tile + R halo)
+    static constexpr int FLOATS = 3 * HT * W + 3 * HV * W;
+};
+
+template <int R, int TZ>
+__global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ StepArgs a)
+{
+    using S = FwdShape<R, TZ>;
+    constexpr int W = S::W, HT = S::HT, HV = S::HV, VW = TX + 2 * R;
+    extern __shared__ float4 smem4[];
+    float *sm = reinterpret_cast<float *>(smem4);
+    float *s_txx = sm, *s_tzz = s_txx + HT * W, *s_txz = s_tzz + HT * W;
+    float *s_vx = s_txz + HT * W, *s_vz = s_vx + HV * W, *s_b = s_vz + HV * W;
+
+    const Grid &g = a.g;
+    const int slot = blockIdx.z, shot = a.shot0 + slot;
+    const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TZ, sx0 = j0 - 2 * R;
+    const float *in = a.in + slot * a.in_stride;
+    float *out = a.out + slot * a.out_stride;
+    const int tid = threadIdx.x;
+    const float dt = a.k.dt;
+
+    for (int e = tid; e < HT * (W / 4); e += NTHREADS) {
+        int r = e / (W / 4), q = e - r * (W / 4);
+        int gi = i0 - 2 * R + r, gj = sx0 + 4 * q;
+        int o = r * W + 4 * q;
+        st4s(s_txx + o, ld4(in + TXX * g.plane, g, gi, gj));
+        st4s(s_tzz + o, ld4(in + TZZ * g.plane, g, gi, gj));
+        st4s(s_txz + o, ld4(in + TXZ * g.plane, g, gi, gj));
+    }
+    for (int e = tid; e < HV * (W / 4); e += NTHREADS) {
+        int r = e / (W / 4), q = e - r * (W / 4);
+        int gi = i0 - R + r, gj = sx0 + 4 * q;
+        int o = r * W + 4 * q;
+        st4s(s_vx + o, ld4(in + VX * g.plane, g, gi, gj));
+        st4s(s_vz + o, ld4(in + VZ * g.plane, g, gi, gj));
+        st4s(s_b + o, ld4(a.mat + 2 * g.plane, g, gi, gj));
+    }
+    __syncthreads();
+    if (a.add_src && tid == 0) {  // wave_propagation.py:652-664, elastic_surface.cl:23-28
+        int si = a.srcz[shot], sj = a.srcx[shot], c = sj - sx0;
+        if (c >= 0 && c < W) {
+            int rt = si - (i0 - 2 * R), rv = si - (i0 - R);
+            if (rt >= 0 && rt < HT) {
+                s_txx[rt * W + c] += a.src.z;
+                s_tzz[rt * W + c] += a.src.w;
+            }
+            if (rv >= 0 && rv < HV) {
+                s_vx[rv * W + c] += a.src.x;
+                s_vz[rv * W + c] += a.src.y;
+            }
+        }
+    }
+    __syncthreads();
+
+    // velocities on the tile plus an R-cell ring (update_velx / update_velz)
+    for (int e = tid; e < HV * VW; e += NTHREADS) {
+        int r = e / VW, cc = e - r * VW;
+        int gi = i0 - R + r, gj = j0 - R + cc;
+        if (!in_domain(g, R, gi, gj)) continue;  // outside: keeps its value
+        int iv = r * W + cc + R, it = iv + R * W;
+        float d = __ldg(a.dampx + gj + XO) + __ldg(a.dampz + gi + ZO);
+        float b = s_b[iv];
+        float vx = s_vx[iv] + dt * (b * (dbwd<R>(s_txx, it, 1, a.k.cx) + dbwd<R>(s_txz, it, W, a.k.cz)));
+        vx = vx + dt * (-d * vx);
+        float vz = s_vz[iv] + dt * (b * (dfwd<R>(s_tzz, it, W, a.k.cz) + dfwd<R>(s_txz, it, 1, a.k.cx)));
+        vz = vz + dt * (-d * vz);
+        s_vx[iv] = vx;
+        s_vz[iv] = vz;
+    }
+    __syncthreads();
+
+    // stresses on the tile (update_tauz / update_tauxz), one column per thread
+    const int c = tid % TX;
+    const int gj = j0 + c;
+    if (gj >= g.tnx) return;
+    for (int r = tid / TX; r < TZ; r += NTHREADS / TX) {
+        int gi = i0 + r;
+        if (gi >= g.tnz) break;
+        int iv = (r + R) * W + c + 2 * R, it = iv + R * W;
+        float txx = s_txx[it], tzz = s_tzz[it], txz = s_txz[it];
+        long long co = cell_off(g, gi, gj);
+        if (in_domain(g, R, gi, gj)) {
+            float lam = __ldg(a.mat + co), mu = __ldg(a.mat + g.plane + co);
+            float d = __ldg(a.dampx + gj + XO) + __ldg(a.dampz + gi + ZO);
+            float dxp_vx = dfwd<R>(s_vx, iv, 1, a.k.cx), dzm_vz = dbwd<R>(s_vz, iv, W, a.k.cz);
+            float dxm_vz = dbwd<R>(s_vz, iv, 1, a.k.cx), dzp_vx = dfwd<R>(s_vx, iv, W, a.k.cz);
+            float l2m = lam + 2.f * mu;
+            txx = txx + dt * (l2m * dxp_vx + lam * dzm_vz);
+            tzz = tzz + dt * (l2m * dzm_vz + lam * dxp_vx);
+            txx = txx + dt * (-d * txx);
+            tzz = tzz + dt * (-d * tzz);
+            txz = txz + dt * (mu * (dxm_vz + dzp_vx));
+            txz = txz + dt * (-d * txz);
+        }
+        out[VX * g.plane + co] = s_vx[iv];
+        out[VZ * g.plane + co] = s_vz[iv];
+        out[TXX * g.plane + co] = txx;
+        out[TZZ * g.plane + co] = tzz;
+        out[TXZ * g.plane + co] = txz;
+        if (a.rec_row >= 0) record_cell(a, in, shot, gi, gj);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// reverse-time step: stresses then velocities, coeff = -1 (elastic.cl:175-306,
+// order of wave_propagation.py:782-812).  Used only by the reference's
+// chpr < 100 checkpoint scheme.
+// ---------------------------------------------------------------------------
+template <int R, int TZ>
+struct RevShape {
+    static constexpr int W = TX + 4 * R;
+    static constexpr int HT = TZ + 4 * R;  // velocity rows
+    static constexpr int HV = TZ + 2 * R;  // stress rows
+    static constexpr int FLOATS = 2 * HT * W + 5 * HV * W;
+};
+
+template <int R, int TZ>
+__global__ void __launch_bounds__(NTHREADS) rev_step(const __grid_constant__ StepArgs a)
+{
+    using S = RevShape<R, TZ>;
+    constexpr int W = S::W, HT = S::HT, HV = S::HV, VW = TX + 2 * R;
+    extern __shared__ float4 smem4[];
+    float *sm = reinterpret_cast<float *>(smem4);
+    float *s_vx = sm, *s_vz = s_vx + HT * W;
+    float *s_txx = s_vz + HT * W, *s_tzz = s_txx + HV * W, *s_txz = s_tzz + HV * W;
+    float *s_lam = s_txz + HV * W, *s_mu = s_lam + HV * W;
+
+    const Grid &g = a.g;
+    const int slot = blockIdx.z;
+    const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TZ, sx0 = j0 - 2 * R;
+    const float *in = a.in + slot * a.in_stride;
+    float *out = a.out + slot * a.out_stride;
+    const int tid = threadIdx.x;
+    const float dt = a.k.dt;
+
+    for (int e = tid; e < HT * (W / 4); e += NTHREADS) {
+        int r = e / (W / 4), q = e - r * (W / 4);
+        int gi = i0 - 2 * R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
+        st4s(s_vx + o, ld4(in + VX * g.plane, g, gi, gj));
+        st4s(s_vz + o, ld4(in + VZ * g.plane, g, gi, gj));
+    }
+    for (int e = tid; e < HV * (W / 4); e += NTHREADS) {
+        int r = e / (W / 4), q = e - r * (W / 4);
+        int gi = i0 - R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
+        st4s(s_txx + o, ld4(in + TXX * g.plane, g, gi, gj));
+        st4s(s_tzz + o, ld4(in + TZZ * g.plane, g, gi, gj));
+        st4s(s_txz + o, ld4(in + TXZ * g.plane, g, gi, gj));
+        st4s(s_lam + o, ld4(a.mat, g, gi, gj));
+        st4s(s_mu + o, ld4(a.mat + g.plane, g, gi, gj));
+    }
+    __syncthreads();
+
+    for (int e = tid; e < HV * VW; e += NTHREADS) {
+        int r = e / VW, cc = e - r * VW;
+        int gi = i0 - R + r, gj = j0 - R + cc;
+        if (!in_domain(g, R, gi, gj)) continue;
+        int is = r * W + cc + R, iv = is + R * W;
+        float d = __ldg(a.dampx + gj + XO) + __ldg(a.dampz + gi + ZO);
+        float lam = s_lam[is], mu = s_mu[is], l2m = lam + 2.f * mu;
+        float dxp_vx = dfwd<R>(s_vx, iv, 1, a.k.cx), dzm_vz = dbwd<R>(s_vz, iv, W, a.k.cz);
+        float dxm_vz = dbwd<R>(s_vz, iv, 1, a.k.cx), dzp_vx = dfwd<R>(s_vx, iv, W, a.k.cz);
+        float txz = s_txz[is];
+        txz = txz - dt * (d * txz);
+        txz = txz - dt * (mu * (dxm_vz + dzp_vx));
+        float txx = s_txx[is], tzz = s_tzz[is];
+        txx = txx - dt * (d * txx);
+        tzz = tzz - dt * (d * tzz);
+        txx = txx - dt * (l2m * dxp_vx + lam * dzm_vz);
+        tzz = tzz - dt * (l2m * dzm_vz + lam * dxp_vx);
+        s_txx[is] = txx;
+        s_tzz[is] = tzz;
+        s_txz[is] = txz;
+    }
+    __syncthreads();
+
+    const int c = tid % TX;
+    const int gj = j0 + c;
+    if (gj >= g.tnx) return;
+    for (int r = tid / TX; r < TZ; r += NTHREADS / TX) {
+        int gi = i0 + r;
+        if (gi >= g.tnz) break;
+        int is = (r + R) * W + c + 2 * R, iv = is + R * W;
+        float vx = s_vx[iv], vz = s_vz[iv];
+        long long co = cell_off(g, gi, gj);
+        if (in_domain(g, R, gi, gj)) {
+            float b = __ldg(a.mat + 2 * g.plane + co);
+            float d = __ldg(a.dampx + gj + XO) + __ldg(a.dampz + gi + ZO);
+            vz = vz - dt * (d * vz);
+            vz = vz - dt * (b * (dfwd<R>(s_tzz, is, W, a.k.cz) + dfwd<R>(s_txz, is, 1, a.k.cx)));
+            vx = vx - dt * (d * vx);
+            vx = vx - dt * (b * (dbwd<R>(s_txx, is, 1, a.k.cx) + dbwd<R>(s_txz, is, W, a.k.cz)));
+        }
+        out[VX * g.plane + co] = vx;
+        out[VZ * g.plane + co] = vz;
+        out[TXX * g.plane + co] = s_txx[is];
+        out[TZZ * g.plane + co] = s_tzz[is];
+        out[TXZ * g.plane + co] = s_txz[is];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// adjoint step + imaging (Adj_injSrc, Adj_update_tau, Adj_update_v, Grad:
+// elastic_surface.cl:48-71, elastic.cl:316-526)
+// ---------------------------------------------------------------------------
+template <int R, int TZ>
+struct AdjShape {
+    static constexpr int W = TX + 4 * R;
+    static constexpr int HT = TZ + 4 * R;  // adjoint velocity + buoyancy rows
+    static constexpr int HV = TZ + 2 * R;  // adjoint stress + lam/mu rows
+    static constexpr int FLOATS = 3 * HT * W + 5 * HV * W;
+};
+
+// Add the residual of one line to the shared arrays.  Velocity components go
+// to rows [i0-2R, ...) (ht rows), stresses to rows [i0-R, ...) (hv rows).
+template <int R, int TZ>
+__device__ __forceinline__ void inject_line(const AdjArgs &a, int l, int shot, int i0, int sx0, float *s_avx,
+                                            float *s_avz, float *s_atx, float *s_atz, float *s_atxz)
+{
+    using S = AdjShape<R, TZ>;
+    constexpr int W = S::W, HT = S::HT, HV = S::HV;
+    const Lines &L = a.lines;
+    // receivers of this line inside the shared window, one per thread
+    int lo, hi;  // k range
+    if (L.drow[l] == 0) {
+        int rr = L.row0[l] - (i0 - 2 * R);
+        if (rr < 0 || rr >= HT) return;
+        int d0 = sx0 - L.col0[l], d1 = sx0 + W - 1 - L.col0[l];
+        lo = d0 <= 0 ? 0 : (d0 + L.dcol[l] - 1) / L.dcol[l];
+        hi = d1 < 0 ? -1 : d1 / L.dcol[l];
+    } else {
+        int cc = L.col0[l] - sx0;
+        if (cc < 0 || cc >= W) return;
+        int d0 = (i0 - 2 * R) - L.row0[l], d1 = (i0 - 2 * R) + HT - 1 - L.row0[l];
+        lo = d0 <= 0 ? 0 : (d0 + L.drow[l] - 1) / L.drow[l];
+        hi = d1 < 0 ? -1 : d1 / L.drow[l];
+    }
+    if (hi > L.count[l] - 1) hi = L.count[l] - 1;
+    for (int k = lo + (int)threadIdx.x; k <= hi; k += NTHREADS) {
+        int i = L.row0[l] + k * L.drow[l], j = L.col0[l] + k * L.dcol[l];
+        if (i < 0 || i >= a.g.tnz || j < 0 || j >= a.g.tnx) continue;
+        long long o = (long long)a.inj_row * a.ns * a.nr + (long long)shot * a.nr + L.slot0[l] + k;
+        int cc = j - sx0;
+        int rt = i - (i0 - 2 * R), rv = i - (i0 - R);
+        if (a.res[0]) s_avx[rt * W + cc] += __ldg(a.res[0] + o);
+        if (a.res[1]) s_avz[rt * W + cc] += __ldg(a.res[1] + o);
+        if (rv >= 0 && rv < HV) {
+            if (a.res[2]) s_atx[rv * W + cc] += __ldg(a.res[2] + o);
+            if (a.res[3]) s_atz[rv * W + cc] += __ldg(a.res[3] + o);
+            if (a.res[4]) s_atxz[rv * W + cc] += __ldg(a.res[4] + o);
+        }
+    }
+}
+
+__device__ __forceinline__ float bf(const __nv_bfloat16 *p, long long i) { return __bfloat162float(p[i]); }
+
+template <int R, int TZ, bool ENERGY>
+__global__ void __launch_bounds__(NTHREADS) adj_step(const __grid_constant__ AdjArgs a)
+{
+    using S = AdjShape<R, TZ>;
+    constexpr int W = S::W, HT = S::HT, HV = S::HV, VW = TX + 2 * R;
+    extern __shared__ float4 smem4[];
+    float *sm = reinterpret_cast<float *>(smem4);
+    float *s_avx = sm, *s_avz = s_avx + HT * W, *s_b = s_avz + HT * W;
+    float *s_atx = s_b + HT * W, *s_atz = s_atx + HV * W, *s_atxz = s_atz + HV * W;
+    float *s_lam = s_atxz + HV * W, *s_mu = s_lam + HV * W;
+
+    const Grid &g = a.g;
+    const int slot = blockIdx.z, shot = a.shot0 + slot;
+    const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TZ, sx0 = j0 - 2 * R;
+    const float *in = a.in + slot * a.in_stride;
+    float *out = a.out + slot * a.out_stride;
+    const int tid = threadIdx.x;
+    const float dt = a.k.dt;
+
+    for (int e = tid; e < HT * (W / 4); e += NTHREADS) {
+        int r = e / (W / 4), q = e - r * (W / 4);
+        int gi = i0 - 2 * R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
+        st4s(s_avx + o, ld4(in + VX * g.plane, g, gi, gj));
+        st4s(s_avz + o, ld4(in + VZ * g.plane, g, gi, gj));
+        st4s(s_b + o, ld4(a.mat + 2 * g.plane, g, gi, gj));
+    }
+    for (int e = tid; e < HV * (W / 4); e += NTHREADS) {
+        int r = e / (W / 4), q = e - r * (W / 4);
+        int gi = i0 - R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
+        st4s(s_atx + o, ld4(in + TXX * g.plane, g, gi, gj));
+        st4s(s_atz + o, ld4(in + TZZ * g.plane, g, gi, gj));
+        st4s(s_atxz + o, ld4(in + TXZ * g.plane, g, gi, gj));
+        st4s(s_lam + o, ld4(a.mat, g, gi, gj));
+        st4s(s_mu + o, ld4(a.mat + g.plane, g, gi, gj));
+    }
+    __syncthreads();
+    if (a.inj_row >= 0) {
+        for (int l = 0; l < a.lines.n; ++l) {
+            inject_line<R, TZ>(a, l, shot, i0, sx0, s_avx, s_avz, s_atx, s_atz, s_atxz);
+            __syncthreads();
+        }
+    }
+
+    // adjoint stresses on the tile plus an R-cell ring (Adj_update_tau)
+    for (int e = tid; e < HV * VW; e += NTHREADS) {
+        int r = e / VW, cc = e - r * VW;
+        int gi = i0 - R + r, gj = j0 - R + cc;
+        if (!in_domain(g, R, gi, gj)) continue;
+        int is = r * W + cc + R, iv = is + R * W;
+        float dx = __ldg(a.dampx + gj + XO), dz = __ldg(a.dampz + gi + ZO);
+        float atx = s_atx[is], atz = s_atz[is], atxz = s_atxz[is];
+        atx = atx + (-dt) * (dx * atx + dfwd_p<R>(s_avx, s_b, iv, 1, a.k.cx));
+        atz = atz + (-dt) * (dz * atz + dbwd_p<R>(s_avz, s_b, iv, W, a.k.cz));
+        atxz = atxz + (-dt) * ((dx + dz) * atxz +
+                               (dfwd_p<R>(s_avx, s_b, iv, W, a.k.cz) + dbwd_p<R>(s_avz, s_b, iv, 1, a.k.cx)));
+        s_atx[is] = atx;
+        s_atz[is] = atz;
+        s_atxz[is] = atxz;
+    }
+    __syncthreads();
+
+    // adjoint velocities on the tile (Adj_update_v) and imaging (Grad)
+    const int c = tid % TX;
+    const int gj = j0 + c;
+    if (gj >= g.tnx) return;
+    const int glo = a.npml + R;
+    const float *F = a.fwd ? a.fwd + slot * a.fwd_stride : nullptr;
+    const __nv_bfloat16 *F16 = a.fwd16 ? a.fwd16 + slot * a.fwd_stride : nullptr;
+    float *G = a.gacc + slot * a.gacc_stride;
+    for (int r = tid / TX; r < TZ; r += NTHREADS / TX) {
+        int gi = i0 + r;
+        if (gi >= g.tnz) break;
+        int is = (r + R) * W + c + 2 * R, iv = is + R * W;
+        float avx = s_avx[iv], avz = s_avz[iv];
+        long long co = cell_off(g, gi, gj);
+        if (in_domain(g, R, gi, gj)) {
+            float dx = __ldg(a.dampx + gj + XO), dz = __ldg(a.dampz + gi + ZO);
+            float sx = dbwd_l2m<R>(s_lam, s_mu, s_atx, is, 1, a.k.cx) + dbwd_p<R>(s_lam, s_atz, is, 1, a.k.cx) +
+                       dbwd_p<R>(s_mu, s_atxz, is, W, a.k.cz);
+            float sz = dfwd_p<R>(s_lam, s_atx, is, W, a.k.cz) + dfwd_l2m<R>(s_lam, s_mu, s_atz, is, W, a.k.cz) +
+                       dfwd_p<R>(s_mu, s_atxz, is, 1, a.k.cx);
+            avx = avx + (-dt) * ((2.f * dx + dz) * avx + sx);
+            avz = avz + (-dt) * ((dx + 2.f * dz) * avz + sz);
+        }
+        float atx = s_atx[is], atz = s_atz[is], atxz = s_atxz[is];
+        out[VX * g.plane + co] = avx;
+        out[VZ * g.plane + co] = avz;
+        out[TXX * g.plane + co] = atx;
+        out[TZZ * g.plane + co] = atz;
+        out[TXZ * g.plane + co] = atxz;
+
+        if (gi < glo || gi > g.tnz - R - a.npml || gj < glo || gj > g.tnx - R - a.npml) continue;
+        const long long P = g.plane, sz_ = g.pitch;
+        float dzp_vx, dxm_vz, dxp_vx, dzm_vz, dzp_tz, dxm_tx, dxp_txz, dzm_txz;
+        float vx = 0.f, vz = 0.f, tx = 0.f, tz = 0.f, txz = 0.f;
+        if (F) {
+            // DzpVx is formed from vz, as the reference does (elastic.cl:485)
+            dzp_vx = gfwd<R>(F + VZ * P, co, sz_, a.k.cz);
+            dxm_vz = gbwd<R>(F + VZ * P, co, 1, a.k.cx);
+            dxp_vx = gfwd<R>(F + VX * P, co, 1, a.k.cx);
+            dzm_vz = gbwd<R>(F + VZ * P, co, sz_, a.k.cz);
+            dzp_tz = gfwd<R>(F + TZZ * P, co, sz_, a.k.cz);
+            dxm_tx = gbwd<R>(F + TXX * P, co, 1, a.k.cx);
+            dxp_txz = gfwd<R>(F + TXZ * P, co, 1, a.k.cx);
+            dzm_txz = gbwd<R>(F + TXZ * P, co, sz_, a.k.cz);
+            if (ENERGY) {
+                vx = F[VX * P + co];
+                vz = F[VZ * P + co];
+                tx = F[TXX * P + co];
+                tz = F[TZZ * P + co];
+                txz = F[TXZ * P + co];
+            }
+        } else {
+#define B16F(f, k) bf(F16 + (f) * P, (k))
+#define BFWD(f, s)                                                                                       \
+    (a.k.c##s[0] * (B16F(f, co + st) - B16F(f, co)) + a.k.c##s[1] * (B16F(f, co + 2 * st) - B16F(f, co - st)) + \
+     (R == 4 ? a.k.c##s[2] * (B16F(f, co + 3 * st) - B16F(f, co - 2 * st)) +                              \
+                   a.k.c##s[3] * (B16F(f, co + 4 * st) - B16F(f, co - 3 * st))                            \
+             : 0.f))
+#define BBWD(f, s)                                                                                       \
+    (a.k.c##s[0] * (B16F(f, co) - B16F(f, co - st)) + a.k.c##s[1] * (B16F(f, co + st) - B16F(f, co - 2 * st)) + \
+     (R == 4 ? a.k.c##s[2] * (B16F(f, co + 2 * st) - B16F(f, co - 3 * st)) +                              \
+                   a.k.c##s[3] * (B16F(f, co + 3 * st) - B16F(f, co - 4 * st))                            \
+             : 0.f))
+            long long st = sz_;
+            dzp_vx = BFWD(VZ, z);
+            dzm_vz = BBWD(VZ, z);
+            dzp_tz = BFWD(TZZ, z);
+            dzm_txz = BBWD(TXZ, z);
+            st = 1;
+            dxm_vz = BBWD(VZ, x);
+            dxp_vx = BFWD(VX, x);
+            dxm_tx = BBWD(TXX, x);
+            dxp_txz = BFWD(TXZ, x);
+            if (ENERGY) {
+                vx = B16F(VX, co);
+                vz = B16F(VZ, co);
+                tx = B16F(TXX, co);
+                tz = B16F(TZZ, co);
+                txz = B16F(TXZ, co);
+            }
+#undef B16F
+#undef BFWD
+#undef BBWD
+        }
+        float b = s_b[iv];
+        float gmu = G[0 * P + co], glam = G[1 * P + co], grho = G[2 * P + co];
+        gmu += 2.f * dt * (atx * dxp_vx + atz * dzm_vz) + dt * atxz * (dzp_vx + dxm_vz);
+        glam += dt * (atx + atz) * (dxp_vx + dzm_vz);
+        grho += -(dt * (b * b)) * (avx * (dxm_tx + dzm_txz) + avz * (dzp_tz + dxp_txz));
+        G[0 * P + co] = gmu;
+        G[1 * P + co] = glam;
+        G[2 * P + co] = grho;
+        if (ENERGY) {
+            float dt2 = dt * dt;
+            G[3 * P + co] += 4.f * dt2 * (tx * tx * dxp_vx * dxp_vx + tz * tz * dzm_vz * dzm_vz) +
+                             dt2 * txz * txz * (dzp_vx * dzp_vx + dxm_vz * dxm_vz);
+            G[4 * P + co] += dt2 * (tx * tx + tz * tz) * (dxp_vx * dxp_vx + dzm_vz * dzm_vz);
+            G[5 * P + co] += dt2 * (vx * vx * (dxm_tx * dxm_tx + dzm_txz * dzm_txz) +
+                                    vz * vz * (dzp_tz * dzp_tz + dxp_txz * dxp_txz));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// set-up and post-processing kernels
+// ---------------------------------------------------------------------------
+
+// max(vp) as the bits of a non-negative float (atomicMax on int orders them).
+__global__ void vp_max_kernel(const float *vp, long long n, int *out_bits)
+{
+    float m = 0.f;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        m = fmaxf(m, vp[k]);
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out_bits, __float_as_int(m));
+}
+
+// Materials of the padded grid (fwi_tools.py:776-811 padding,
+// wave_propagation.py:575-591).  float32 with explicit rounding so the
+// values match numpy's elementwise float32 results bit for bit.
+__global__ void model_kernel(Grid g, int nz, int nx, int npml, const float *vp, const float *vs, const float *rho,
+                             float *mat)
+{
+    long long n = (long long)g.tnz * g.tnx;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(k / g.tnx), j = (int)(k - (long long)i * g.tnx);
+        int mi = min(max(i - npml, 0), nz - 1), mj = min(max(j - npml, 0), nx - 1);
+        long long m = (long long)mi * nx + mj;
+        float p = vp[m], s = vs[m], r = rho[m];
+        float mu = __fmul_rn(r, __fmul_rn(s, s));
+        float lam = __fsub_rn(__fmul_rn(r, __fmul_rn(p, p)), __fmul_rn(2.f, mu));
+        long long c = cell_off(g, i, j);
+        mat[c] = lam;
+        mat[g.plane + c] = mu;
+        mat[2 * g.plane + c] = __frcp_rn(r);
+        mat[3 * g.plane + c] = r;
+    }
+}
+
+__global__ void damp_kernel(Grid g, const float *damp_x, const float *damp_z, const int *vpmax_bits, float *dampx,
+                            float *dampz)
+{
+    float vmax = __int_as_float(*vpmax_bits);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.pitch + g.rows; k += gridDim.x * blockDim.x) {
+        if (k < g.pitch) {
+            int j = k - XO;
+            dampx[k] = (j >= 0 && j < g.tnx) ? __fmul_rn(damp_x[j], vmax) : 0.f;
+        } else {
+            int i = k - g.pitch - ZO;
+            dampz[k - g.pitch] = (i >= 0 && i < g.tnz) ? __fmul_rn(damp_z[i], vmax) : 0.f;
+        }
+    }
+}
+
+// Sum the per-slot accumulators into slot 0: G0 += G1 + ... (shot order).
+__global__ void reduce_slots_kernel(float *gacc, long long slot_stride, int nslots, long long n)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        float s = gacc[k];
+        for (int q = 1; q < nslots; ++q) s += gacc[q * slot_stride + k];
+        gacc[k] = s;
+    }
+}
+
+// Copy the padded accumulators out as dense [nacc][tnz][tnx].
+__global__ void raw_out_kernel(Grid g, const float *gacc, int nacc, float *raw)
+{
+    long long n = (long long)g.tnz * g.tnx;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n * nacc;
+         k += (long long)gridDim.x * blockDim.x) {
+        int q = (int)(k / n);
+        long long r = k - q * n;
+        int i = (int)(r / g.tnx), j = (int)(r - (long long)i * g.tnx);
+        raw[k] = gacc[q * g.plane + cell_off(g, i, j)];
+    }
+}
+
+// Energy-balancing factor 1/sqrt(P) inside the window, its max |.| as bits.
+struct PostArgs {
+    Grid g;
+    int nz, nx, npml;
+    int r0, r1, c0, c1;  // window (model grid)
+    int energy;
+    int param;           // 0 lmd, 1 dv
+    const float *gacc;   // slot 0 accumulators
+    const float *mat;
+    int *fmax_bits;      // [3] max factor per gradient (Gmu, Glam, Grho order)
+    float *out;          // [3][nz][nx]
+};
+
+__device__ __forceinline__ float window_factor(const PostArgs &a, int q, int i, int j)
+{
+    // q: 0 Gmu, 1 Glam, 2 Grho ; returns 1/sqrt(P) (or 1) inside, 0 outside
+    if (i < a.r0 || i >= a.r1 || j < a.c0 || j >= a.c1) return 0.f;
+    if (!a.energy) return 1.f;
+    float p = a.gacc[(3 + q) * a.g.plane + cell_off(a.g, i + a.npml, j + a.npml)];
+    return __fdiv_rn(1.f, __fsqrt_rn(p));
+}
+
+__global__ void factor_max_kernel(PostArgs a)
+{
+    float m[3] = {0.f, 0.f, 0.f};
+    long long n = (long long)a.nz * a.nx;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(k / a.nx), j = (int)(k - (long long)i * a.nx);
+        for (int q = 0; q < 3; ++q) m[q] = fmaxf(m[q], fabsf(window_factor(a, q, i, j)));
+    }
+    for (int q = 0; q < 3; ++q) {
+        float v = m[q];
+        for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if ((threadIdx.x & 31) == 0) atomicMax(a.fmax_bits + q, __float_as_int(v));
+    }
+}
+
+// gradient_reading + grad_lmd_to_vd (wave_propagation.py:279-331,
+// grad_switcher.py:331-383) with numpy's float32 operation order.
+__global__ void post_kernel(PostArgs a)
+{
+    long long n = (long long)a.nz * a.nx;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(k / a.nx), j = (int)(k - (long long)i * a.nx);
+        long long c = cell_off(a.g, i + a.npml, j + a.npml);
+        float gm = a.gacc[0 * a.g.plane + c], gl = a.gacc[1 * a.g.plane + c], gr = a.gacc[2 * a.g.plane + c];
+        float fmu = __fdiv_rn(window_factor(a, 0, i, j), __int_as_float(a.fmax_bits[0]));
+        float flam = __fdiv_rn(window_factor(a, 1, i, j), __int_as_float(a.fmax_bits[1]));
+        float frho = __fdiv_rn(window_factor(a, 2, i, j), __int_as_float(a.fmax_bits[2]));
+        float glam = __fmul_rn(gl, flam), gmu = __fmul_rn(gm, fmu), grho = __fmul_rn(gr, frho);
+        if (a.param == 0) {
+            a.out[k] = glam;
+            a.out[n + k] = gmu;
+            a.out[2 * n + k] = grho;
+            continue;
+        }
+        float lam = a.mat[c], mu = a.mat[a.g.plane + c], rho = a.mat[3 * a.g.plane + c];
+        float vp = __fsqrt_rn(__fdiv_rn(__fadd_rn(lam, __fmul_rn(2.f, mu)), rho));
+        float vs = __fsqrt_rn(__fdiv_rn(mu, rho));
+        float vs2 = __fmul_rn(vs, vs);
+        float vpvs = __fsub_rn(__fmul_rn(vp, vp), __fmul_rn(2.f, __fmul_rn(vs, vs)));
+        float gvp = __fadd_rn(__fadd_rn(__fmul_rn(__fmul_rn(__fmul_rn(glam, 2.f), vp), rho), __fmul_rn(gmu, 0.f)),
+                              __fmul_rn(grho, 0.f));
+        float gvs = __fadd_rn(__fadd_rn(__fmul_rn(glam, __fmul_rn(__fmul_rn(-4.f, rho), vs)),
+                                        __fmul_rn(__fmul_rn(__fmul_rn(gmu, 2.f), vs), rho)),
+                              __fmul_rn(grho, 0.f));
+        float grr = __fadd_rn(__fadd_rn(__fmul_rn(glam, vpvs), __fmul_rn(gmu, vs2)), grho);
+        a.out[k] = gvp;
+        a.out[n + k] = gvs;
+        a.out[2 * n + k] = grr;
+    }
+}
+
+// res = est - obs; misfit += 0.5 * sum(res^2)
+__global__ void l2_kernel(const float *est, const float *obs, float *res, long long n, double *misfit)
+{
+    double acc = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        float r = __fsub_rn(est[k], obs[k]);
+        res[k] = r;
+        acc += (double)r * (double)r;
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(misfit, 0.5 * acc);
+}
+
+__global__ void mean2_kernel(const float *a, const float *b, float *out, long long n)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        out[k] = __fdiv_rn(__fadd_rn(a[k], b[k]), 2.f);
+}
+
+}  // namespace pyfwi

@@ -1,0 +1,653 @@
+// Host side of libpyfwi_b200: plans, workspace layout, the time-loop
+// schedules, and the C ABI declared in include/pyfwi_b200.h.
+//
+// The reference drives its kernels from Python, one pyopencl launch per
+// kernel, step and shot (PyFWI src/PyFWI/wave_propagation.py:625-856).  Here a
+// plan runs every step of a batch of shots with one fused launch per step,
+// all enqueued on the caller's stream (optionally replayed as a CUDA graph).
+#include "pyfwi_b200.h"
+#include "kernels.cuh"
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace pyfwi;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(x)                                                                               \
+    do {                                                                                    \
+        cudaError_t e_ = (x);                                                               \
+        if (e_ != cudaSuccess) return fail(PYFWI_E_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
+    } while (0)
+
+#define CKL()                                                                                      \
+    do {                                                                                           \
+        cudaError_t e_ = cudaGetLastError();                                                       \
+        if (e_ != cudaSuccess) return fail(PYFWI_E_CUDA, "kernel launch: %s", cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr size_t ALIGN = 256;
+size_t up(size_t x, size_t a = ALIGN) { return (x + a - 1) / a * a; }
+
+// tile variants: rows per tile
+constexpr int TILE_TZ[] = {16, 8, 32};
+constexpr int N_TILES = 3;
+
+}  // namespace
+
+struct pyfwi_plan {
+    pyfwi_geometry geom;
+    pyfwi_options opt;
+    std::vector<int32_t> srcx, srcz, chp;
+    std::vector<float> src_vals;  // [n_inj][4] host copy of the last forward's wavelet
+    Grid g;
+    Coef k;
+    Lines lines;
+    int R, tz, nacc, G, ngroups, seg, M, n_inj;
+    long long state;  // floats per state (5 planes)
+    // workspace offsets in bytes
+    size_t o_hdr, o_src, o_mat, o_dampx, o_dampz, o_work, o_adj, o_gacc, o_store, o_store16, total;
+    long long launches = 0;
+    bool model_set = false, fwd_valid = false;
+    void *ws_initialised = nullptr;
+};
+
+namespace {
+
+int check_ws(const pyfwi_plan *p, void *ws, size_t bytes)
+{
+    if (!ws) return fail(PYFWI_E_WORKSPACE, "workspace is NULL");
+    if (bytes < p->total) return fail(PYFWI_E_WORKSPACE, "workspace has %zu bytes, plan needs %zu", bytes, p->total);
+    if (reinterpret_cast<uintptr_t>(ws) % ALIGN) return fail(PYFWI_E_WORKSPACE, "workspace not 256-byte aligned");
+    return PYFWI_OK;
+}
+
+template <typename T>
+T *at(void *ws, size_t off)
+{
+    return reinterpret_cast<T *>(static_cast<char *>(ws) + off);
+}
+
+// ---- kernel dispatch ------------------------------------------------------
+template <int R, int TZ>
+int launch_fwd(pyfwi_plan *p, const StepArgs &a, int nslots, cudaStream_t s, bool reverse)
+{
+    dim3 grid((p->g.tnx + TX - 1) / TX, (p->g.tnz + TZ - 1) / TZ, nslots);
+    if (!reverse) {
+        size_t sm = FwdShape<R, TZ>::FLOATS * sizeof(float);
+        static bool attr = false;
+        if (!attr) {
+            CK(cudaFuncSetAttribute(fwd_step<R, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            attr = true;
+        }
+        fwd_step<R, TZ><<<grid, NTHREADS, sm, s>>>(a);
+    } else {
+        size_t sm = RevShape<R, TZ>::FLOATS * sizeof(float);
+        static bool attr = false;
+        if (!attr) {
+            CK(cudaFuncSetAttribute(rev_step<R, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            attr = true;
+        }
+        rev_step<R, TZ><<<grid, NTHREADS, sm, s>>>(a);
+    }
+    p->launches++;
+    CKL();
+    return PYFWI_OK;
+}
+
+template <int R, int TZ, bool E>
+int launch_adj_t(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
+{
+    dim3 grid((p->g.tnx + TX - 1) / TX, (p->g.tnz + TZ - 1) / TZ, nslots);
+    size_t sm = AdjShape<R, TZ>::FLOATS * sizeof(float);
+    static bool attr = false;
+    if (!attr) {
+        CK(cudaFuncSetAttribute(adj_step<R, TZ, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        attr = true;
+    }
+    adj_step<R, TZ, E><<<grid, NTHREADS, sm, s>>>(a);
+    p->launches++;
+    CKL();
+    return PYFWI_OK;
+}
+
+template <int R, int TZ>
+int launch_adj(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
+{
+    return p->nacc == 6 ? launch_adj_t<R, TZ, true>(p, a, nslots, s) : launch_adj_t<R, TZ, false>(p, a, nslots, s);
+}
+
+int step_fwd(pyfwi_plan *p, const StepArgs &a, int nslots, cudaStream_t s, bool reverse)
+{
+#define CASE(R_, TZ_) \
+    if (p->R == R_ && p->tz == TZ_) return launch_fwd<R_, TZ_>(p, a, nslots, s, reverse);
+    CASE(2, 16) CASE(2, 8) CASE(2, 32) CASE(4, 16) CASE(4, 8) CASE(4, 32)
+#undef CASE
+    return fail(PYFWI_E_INVALID, "no kernel for half order %d, tile rows %d", p->R, p->tz);
+}
+
+int step_adj(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
+{
+#define CASE(R_, TZ_) \
+    if (p->R == R_ && p->tz == TZ_) return launch_adj<R_, TZ_>(p, a, nslots, s);
+    CASE(2, 16) CASE(2, 8) CASE(2, 32) CASE(4, 16) CASE(4, 8) CASE(4, 32)
+#undef CASE
+    return fail(PYFWI_E_INVALID, "no kernel for half order %d, tile rows %d", p->R, p->tz);
+}
+
+int grid_blocks(long long n)
+{
+    long long b = (n + 255) / 256;
+    return (int)(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
+}
+
+// ---- state addressing -------------------------------------------------------
+struct Buf {
+    float *base;       // state of slot 0
+    long long stride;  // floats between slots
+};
+
+// exact mode: where state S_s of the current group lives during a pass
+Buf exact_state(pyfwi_plan *p, void *ws, int s)
+{
+    float *store = at<float>(ws, p->o_store);
+    float *work = at<float>(ws, p->o_work);
+    long long sstride = (long long)(p->M + p->seg) * p->state;
+    if (s == 0) return {store, sstride};
+    if (p->M > 1 && s % p->seg == 0 && s / p->seg <= p->M - 1) return {store + (long long)(s / p->seg) * p->state, sstride};
+    if (s > (p->M - 1) * p->seg) return {store + (long long)(p->M + s - (p->M - 1) * p->seg - 1) * p->state, sstride};
+    return {work + (long long)(s & 1) * p->state, 2 * p->state};
+}
+
+StepArgs base_step(pyfwi_plan *p, void *ws)
+{
+    StepArgs a;
+    memset(&a, 0, sizeof a);
+    a.g = p->g;
+    a.k = p->k;
+    a.mat = at<float>(ws, p->o_mat);
+    a.dampx = at<float>(ws, p->o_dampx);
+    a.dampz = at<float>(ws, p->o_dampz);
+    a.srcx = at<int>(ws, p->o_src);
+    a.srcz = at<int>(ws, p->o_src) + p->geom.ns;
+    a.rec_row = -1;
+    a.lines = p->lines;
+    a.nr = p->geom.nr;
+    a.ns = p->geom.ns;
+    a.trace_plane = (long long)p->geom.nt_ext * p->geom.ns * p->geom.nr;
+    return a;
+}
+
+float4 src_at(const pyfwi_plan *p, int inj)
+{
+    if (inj < 0 || inj >= (int)(p->src_vals.size() / 4)) return make_float4(0.f, 0.f, 0.f, 0.f);
+    const float *v = &p->src_vals[4 * (size_t)inj];
+    return make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// One forward pass of a group (exact mode), optionally recording traces.
+int exact_pass(pyfwi_plan *p, void *ws, int s0, int n, float *traces, cudaStream_t st)
+{
+    Buf z = exact_state(p, ws, 0);
+    for (int q = 0; q < n; ++q) CK(cudaMemsetAsync(z.base + q * z.stride, 0, p->state * sizeof(float), st));
+    StepArgs a = base_step(p, ws);
+    a.shot0 = s0;
+    a.traces = traces;
+    for (int t = 0; t < p->geom.nt; ++t) {
+        Buf in = exact_state(p, ws, t), out = exact_state(p, ws, t + 1);
+        a.in = in.base;
+        a.in_stride = in.stride;
+        a.out = out.base;
+        a.out_stride = out.stride;
+        bool inj = t % p->geom.dt_scale == 0;
+        int k = t / p->geom.dt_scale;
+        a.add_src = inj;
+        a.src = src_at(p, k);
+        a.rec_row = (inj && traces && k < p->geom.nt_ext) ? k : -1;
+        int rc = step_fwd(p, a, n, st, false);
+        if (rc) return rc;
+    }
+    return PYFWI_OK;
+}
+
+// reverse mode: checkpoint slot k of the group
+Buf chp_state(pyfwi_plan *p, void *ws, int s0, int k)
+{
+    float *store = at<float>(ws, p->o_store);
+    long long stride = (long long)p->chp.size() * p->state;
+    return {store + (long long)s0 * stride + (long long)k * p->state, stride};
+}
+
+Buf work_state(pyfwi_plan *p, void *ws, int w)
+{
+    return {at<float>(ws, p->o_work) + (long long)w * p->state, 2 * p->state};
+}
+
+int reverse_pass(pyfwi_plan *p, void *ws, int s0, int n, float *traces, cudaStream_t st)
+{
+    // states stored after the steps listed in chp (wave_propagation.py:710-727)
+    Buf cur = work_state(p, ws, 0);
+    for (int q = 0; q < n; ++q) CK(cudaMemsetAsync(cur.base + q * cur.stride, 0, p->state * sizeof(float), st));
+    int wcur = 0;  // work buffer holding the current state (-1: a checkpoint slot)
+    size_t kc = 0;
+    StepArgs a = base_step(p, ws);
+    a.shot0 = s0;
+    a.traces = traces;
+    for (int t = 0; t < p->geom.nt; ++t) {
+        Buf out;
+        int wnext;
+        if (kc < p->chp.size() && p->chp[kc] == t) {
+            out = chp_state(p, ws, s0, (int)kc);
+            ++kc;
+            wnext = -1;
+        } else {
+            wnext = wcur == 0 ? 1 : 0;
+            out = work_state(p, ws, wnext);
+        }
+        a.in = cur.base;
+        a.in_stride = cur.stride;
+        a.out = out.base;
+        a.out_stride = out.stride;
+        bool inj = t % p->geom.dt_scale == 0;
+        int k = t / p->geom.dt_scale;
+        a.add_src = inj;
+        a.src = src_at(p, k);
+        a.rec_row = (inj && traces && k < p->geom.nt_ext) ? k : -1;
+        int rc = step_fwd(p, a, n, st, false);
+        if (rc) return rc;
+        cur = out;
+        wcur = wnext;
+    }
+    return PYFWI_OK;
+}
+
+AdjArgs base_adj(pyfwi_plan *p, void *ws, const float *const *res)
+{
+    AdjArgs a;
+    memset(&a, 0, sizeof a);
+    a.g = p->g;
+    a.k = p->k;
+    a.mat = at<float>(ws, p->o_mat);
+    a.dampx = at<float>(ws, p->o_dampx);
+    a.dampz = at<float>(ws, p->o_dampz);
+    a.npml = p->geom.npml;
+    a.gacc = at<float>(ws, p->o_gacc);
+    a.gacc_stride = (long long)p->nacc * p->g.plane;
+    for (int c = 0; c < 5; ++c) a.res[c] = res ? res[c] : nullptr;
+    a.nr = p->geom.nr;
+    a.ns = p->geom.ns;
+    a.lines = p->lines;
+    return a;
+}
+
+// backward iteration t of the reference loop (wave_propagation.py:814-848)
+int adjoint_iter(pyfwi_plan *p, AdjArgs &a, int t, int &t_src, int &ping, float *adj, int n, cudaStream_t st)
+{
+    if (t % p->geom.dt_scale == 0) {
+        int row = t_src - 1;
+        if (row < 0) row += p->geom.nt_ext;  // numpy negative index
+        a.inj_row = row;
+        t_src -= 1;
+    } else {
+        a.inj_row = -1;
+    }
+    a.in = adj + (long long)ping * p->state;
+    a.out = adj + (long long)(1 - ping) * p->state;
+    a.in_stride = a.out_stride = 2 * p->state;
+    int rc = step_adj(p, a, n, st);
+    ping = 1 - ping;
+    return rc;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char *pyfwi_last_error(void) { return g_err.c_str(); }
+
+int pyfwi_abi_version(void) { return PYFWI_ABI_VERSION; }
+
+int pyfwi_tile_count(int32_t half_order) { return (half_order == 2 || half_order == 4) ? N_TILES : 0; }
+
+int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int32_t *srcz, const pyfwi_options *opt,
+                      pyfwi_plan **out)
+{
+    if (!geom || !srcx || !srcz || !opt || !out) return fail(PYFWI_E_INVALID, "NULL argument");
+    *out = nullptr;
+    const pyfwi_geometry &G = *geom;
+    if (G.half_order != 2 && G.half_order != 4) return fail(PYFWI_E_INVALID, "half_order must be 2 or 4");
+    if (G.nz < 1 || G.nx < 1 || G.npml < 0 || G.nt < 1 || G.nt_ext < 1 || G.dt_scale < 1 || G.ns < 1 || G.nr < 1)
+        return fail(PYFWI_E_INVALID, "bad grid/time/shot sizes");
+    if (G.n_lines < 1 || G.n_lines > 3) return fail(PYFWI_E_INVALID, "n_lines must be 1..3");
+    const int tnz = G.nz + 2 * G.npml, tnx = G.nx + 2 * G.npml;
+    for (int l = 0; l < G.n_lines; ++l) {
+        const pyfwi_rec_line &L = G.lines[l];
+        if (L.count < 0 || L.slot0 < 0 || L.slot0 + L.count > G.nr) return fail(PYFWI_E_INVALID, "line %d slots", l);
+        if ((L.drow == 0) == (L.dcol == 0) || L.drow < 0 || L.dcol < 0)
+            return fail(PYFWI_E_INVALID, "line %d: exactly one of drow, dcol must be positive", l);
+    }
+    for (int s = 0; s < G.ns; ++s)
+        if (srcx[s] < 0 || srcx[s] >= tnx || srcz[s] < 0 || srcz[s] >= tnz)
+            return fail(PYFWI_E_INVALID, "source %d at (%d, %d) is outside the %dx%d grid", s, srcz[s], srcx[s], tnz, tnx);
+    if (opt->checkpoint != PYFWI_CKPT_EXACT && opt->checkpoint != PYFWI_CKPT_REVERSE)
+        return fail(PYFWI_E_INVALID, "unknown checkpoint mode");
+    if (opt->checkpoint == PYFWI_CKPT_REVERSE) {
+        if (opt->nchp < 1 || !opt->chp) return fail(PYFWI_E_INVALID, "reverse mode needs a checkpoint list");
+        for (int q = 0; q < opt->nchp; ++q)
+            if (opt->chp[q] < 0 || opt->chp[q] >= G.nt || (q && opt->chp[q] <= opt->chp[q - 1]))
+                return fail(PYFWI_E_INVALID, "checkpoint steps must be increasing and inside [0, nt)");
+        if (opt->chp[opt->nchp - 1] != G.nt - 1) return fail(PYFWI_E_INVALID, "last checkpoint must be step nt-1");
+    }
+    if (opt->snapshot == PYFWI_SNAP_BF16) return fail(PYFWI_E_INVALID, "bf16 snapshots are not enabled in this build");
+    if (opt->tile < 0 || opt->tile >= N_TILES) return fail(PYFWI_E_INVALID, "tile variant out of range");
+
+    pyfwi_plan *p = new pyfwi_plan();
+    p->geom = G;
+    p->opt = *opt;
+    p->srcx.assign(srcx, srcx + G.ns);
+    p->srcz.assign(srcz, srcz + G.ns);
+    if (opt->checkpoint == PYFWI_CKPT_REVERSE) p->chp.assign(opt->chp, opt->chp + opt->nchp);
+    p->opt.chp = nullptr;
+    p->R = G.half_order;
+    p->tz = TILE_TZ[opt->tile];
+    p->nacc = opt->energy ? 6 : 3;
+    p->g.tnz = tnz;
+    p->g.tnx = tnx;
+    p->g.pitch = (int)up((size_t)tnx + 2 * XO, 32);
+    p->g.rows = tnz + 2 * ZO;
+    p->g.plane = (long long)p->g.pitch * p->g.rows;
+    p->state = 5 * p->g.plane;
+    for (int q = 0; q < 4; ++q) {
+        p->k.cx[q] = G.c[q] / G.dh;
+        p->k.cz[q] = G.c[q] / G.dh;
+    }
+    p->k.dt = G.dt;
+    memset(&p->lines, 0, sizeof p->lines);
+    p->lines.n = G.n_lines;
+    for (int l = 0; l < G.n_lines; ++l) {
+        const pyfwi_rec_line &L = G.lines[l];
+        p->lines.row0[l] = L.row0;
+        p->lines.col0[l] = L.col0;
+        p->lines.drow[l] = L.drow;
+        p->lines.dcol[l] = L.dcol;
+        p->lines.count[l] = L.count;
+        p->lines.slot0[l] = L.slot0;
+        p->lines.vzx[l] = L.vz_from_vx;
+    }
+    p->G = opt->shot_batch > 0 && opt->shot_batch < G.ns ? opt->shot_batch : G.ns;
+    p->ngroups = (G.ns + p->G - 1) / p->G;
+    p->seg = opt->segment > 0 && opt->segment < G.nt ? opt->segment : G.nt;
+    p->M = (G.nt + p->seg - 1) / p->seg;
+    p->n_inj = (G.nt + G.dt_scale - 1) / G.dt_scale;
+
+    const size_t pf = (size_t)p->g.plane * sizeof(float), sb = (size_t)p->state * sizeof(float);
+    size_t o = 0;
+    p->o_hdr = o;
+    o += ALIGN;
+    p->o_src = o;
+    o += up(2 * (size_t)G.ns * sizeof(int));
+    p->o_mat = o;
+    o += up(4 * pf);
+    p->o_dampx = o;
+    o += up((size_t)p->g.pitch * sizeof(float));
+    p->o_dampz = o;
+    o += up((size_t)p->g.rows * sizeof(float));
+    p->o_work = o;
+    o += up(2 * sb * p->G);
+    p->o_adj = o;
+    o += up(2 * sb * p->G);
+    p->o_gacc = o;
+    o += up((size_t)p->nacc * pf * p->G);
+    p->o_store = o;
+    if (opt->checkpoint == PYFWI_CKPT_EXACT)
+        o += up((size_t)(p->M + p->seg) * sb * p->G);
+    else
+        o += up(p->chp.size() * sb * G.ns);
+    p->o_store16 = o;
+    p->total = o;
+    *out = p;
+    return PYFWI_OK;
+}
+
+int pyfwi_plan_destroy(pyfwi_plan *plan)
+{
+    delete plan;
+    return PYFWI_OK;
+}
+
+int pyfwi_workspace_size(const pyfwi_plan *p, size_t *bytes)
+{
+    if (!p || !bytes) return fail(PYFWI_E_INVALID, "NULL argument");
+    *bytes = p->total;
+    return PYFWI_OK;
+}
+
+int pyfwi_launch_count(const pyfwi_plan *p, int64_t *count)
+{
+    if (!p || !count) return fail(PYFWI_E_INVALID, "NULL argument");
+    *count = p->launches;
+    return PYFWI_OK;
+}
+
+int pyfwi_set_model(pyfwi_plan *p, void *ws, size_t bytes, const float *vp, const float *vs, const float *rho,
+                    const float *damp_x, const float *damp_z, void *stream)
+{
+    if (!p || !vp || !vs || !rho || !damp_x || !damp_z) return fail(PYFWI_E_INVALID, "NULL argument");
+    int rc = check_ws(p, ws, bytes);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (p->ws_initialised != ws) {
+        // frames and padding of every plane must read as zero
+        CK(cudaMemsetAsync(ws, 0, p->total, st));
+        p->ws_initialised = ws;
+    }
+    CK(cudaMemcpyAsync(at<int>(ws, p->o_src), p->srcx.data(), p->geom.ns * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(at<int>(ws, p->o_src) + p->geom.ns, p->srcz.data(), p->geom.ns * sizeof(int),
+                       cudaMemcpyHostToDevice, st));
+    int *vmax = at<int>(ws, p->o_hdr);
+    CK(cudaMemsetAsync(vmax, 0, sizeof(int), st));
+    long long nm = (long long)p->geom.nz * p->geom.nx;
+    vp_max_kernel<<<grid_blocks(nm), 256, 0, st>>>(vp, nm, vmax);
+    p->launches++;
+    CKL();
+    model_kernel<<<grid_blocks((long long)p->g.tnz * p->g.tnx), 256, 0, st>>>(p->g, p->geom.nz, p->geom.nx, p->geom.npml,
+                                                                              vp, vs, rho, at<float>(ws, p->o_mat));
+    p->launches++;
+    CKL();
+    damp_kernel<<<grid_blocks(p->g.pitch + p->g.rows), 256, 0, st>>>(p->g, damp_x, damp_z, vmax,
+                                                                    at<float>(ws, p->o_dampx), at<float>(ws, p->o_dampz));
+    p->launches++;
+    CKL();
+    p->model_set = true;
+    p->fwd_valid = false;
+    return PYFWI_OK;
+}
+
+int pyfwi_forward(pyfwi_plan *p, void *ws, size_t bytes, const float *src_vals, int32_t n_src, float *traces,
+                  void *stream)
+{
+    if (!p || (n_src > 0 && !src_vals) || n_src < 0) return fail(PYFWI_E_INVALID, "bad argument");
+    int rc = check_ws(p, ws, bytes);
+    if (rc) return rc;
+    if (!p->model_set) return fail(PYFWI_E_STATE, "pyfwi_set_model must come first");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    p->src_vals.assign(src_vals, src_vals + 4 * (size_t)n_src);
+    if (traces)
+        CK(cudaMemsetAsync(traces, 0, 5 * (size_t)p->geom.nt_ext * p->geom.ns * p->geom.nr * sizeof(float), st));
+    for (int grp = 0; grp < p->ngroups; ++grp) {
+        int s0 = grp * p->G, n = std::min(p->G, p->geom.ns - s0);
+        rc = p->opt.checkpoint == PYFWI_CKPT_EXACT ? exact_pass(p, ws, s0, n, traces, st)
+                                                     : reverse_pass(p, ws, s0, n, traces, st);
+        if (rc) return rc;
+    }
+    p->fwd_valid = true;
+    return PYFWI_OK;
+}
+
+int pyfwi_gradient(pyfwi_plan *p, void *ws, size_t bytes, const float *const *residual, int32_t param, float *grad,
+                   float *raw, void *stream)
+{
+    if (!p || !grad || (param != PYFWI_PARAM_LMD && param != PYFWI_PARAM_DV)) return fail(PYFWI_E_INVALID, "bad argument");
+    int rc = check_ws(p, ws, bytes);
+    if (rc) return rc;
+    if (!p->fwd_valid) return fail(PYFWI_E_STATE, "pyfwi_gradient needs a pyfwi_forward of the current model first");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const pyfwi_geometry &G = p->geom;
+    float *gacc = at<float>(ws, p->o_gacc);
+    float *adj = at<float>(ws, p->o_adj);
+    CK(cudaMemsetAsync(gacc, 0, (size_t)p->nacc * p->g.plane * p->G * sizeof(float), st));
+    AdjArgs a = base_adj(p, ws, residual);
+
+    for (int grp = 0; grp < p->ngroups; ++grp) {
+        int s0 = grp * p->G, n = std::min(p->G, G.ns - s0);
+        a.shot0 = s0;
+        for (int q = 0; q < n; ++q) CK(cudaMemsetAsync(adj + 2 * q * p->state, 0, p->state * sizeof(float), st));
+        int ping = 0, t_src = G.nt_ext;
+        if (p->opt.checkpoint == PYFWI_CKPT_EXACT) {
+            if (p->ngroups > 1 || !p->fwd_valid) {
+                rc = exact_pass(p, ws, s0, n, nullptr, st);
+                if (rc) return rc;
+            }
+            StepArgs f = base_step(p, ws);
+            f.shot0 = s0;
+            for (int m = p->M - 1; m >= 0; --m) {
+                int t_lo = m * p->seg, t_hi = std::min((m + 1) * p->seg, G.nt);
+                if (m < p->M - 1) {  // recompute segment m from its restart state
+                    for (int t = t_lo; t < t_hi; ++t) {
+                        Buf in = exact_state(p, ws, t);
+                        Buf out = {at<float>(ws, p->o_store) + (long long)(p->M + t - t_lo) * p->state,
+                                   (long long)(p->M + p->seg) * p->state};
+                        if (t > t_lo)
+                            in = {at<float>(ws, p->o_store) + (long long)(p->M + t - t_lo - 1) * p->state, out.stride};
+                        f.in = in.base;
+                        f.in_stride = in.stride;
+                        f.out = out.base;
+                        f.out_stride = out.stride;
+                        bool inj = t % G.dt_scale == 0;
+                        f.add_src = inj;
+                        f.src = src_at(p, t / G.dt_scale);
+                        f.rec_row = -1;
+                        rc = step_fwd(p, f, n, st, false);
+                        if (rc) return rc;
+                    }
+                }
+                for (int t = t_hi - 1; t >= std::max(t_lo, 1); --t) {
+                    // forward state after step t: S_{t+1}
+                    a.fwd = at<float>(ws, p->o_store) + (long long)(p->M + t - t_lo) * p->state;
+                    a.fwd_stride = (long long)(p->M + p->seg) * p->state;
+                    rc = adjoint_iter(p, a, t, t_src, ping, adj, n, st);
+                    if (rc) return rc;
+                }
+            }
+        } else {
+            // reference chpr < 100 scheme (wave_propagation.py:761-812)
+            int nchp = (int)p->chp.size(), chpc = nchp - 1, wlast = 1;
+            Buf cur = {nullptr, 0};
+            StepArgs f = base_step(p, ws);
+            f.shot0 = s0;
+            for (int t = G.nt - 1; t > 0; --t) {
+                int kk = chpc >= 0 ? chpc : chpc + nchp;
+                if (t == p->chp[kk]) {
+                    cur = chp_state(p, ws, s0, kk);
+                    chpc -= 1;
+                } else {
+                    if (!cur.base) return fail(PYFWI_E_STATE, "reverse schedule has no starting checkpoint");
+                    int w = 1 - wlast;
+                    Buf out = work_state(p, ws, w);
+                    f.in = cur.base;
+                    f.in_stride = cur.stride;
+                    f.out = out.base;
+                    f.out_stride = out.stride;
+                    rc = step_fwd(p, f, n, st, true);
+                    if (rc) return rc;
+                    cur = out;
+                    wlast = w;
+                }
+                a.fwd = cur.base;
+                a.fwd_stride = cur.stride;
+                rc = adjoint_iter(p, a, t, t_src, ping, adj, n, st);
+                if (rc) return rc;
+            }
+        }
+    }
+    if (p->opt.checkpoint == PYFWI_CKPT_EXACT && p->M > 1) p->fwd_valid = false;  // last segment overwritten
+    if (p->opt.checkpoint == PYFWI_CKPT_EXACT && p->ngroups > 1) p->fwd_valid = true;  // passes were redone anyway
+
+    const long long nplane = (long long)p->nacc * p->g.plane;
+    if (p->G > 1) {
+        reduce_slots_kernel<<<grid_blocks(nplane), 256, 0, st>>>(gacc, nplane, p->G, nplane);
+        p->launches++;
+        CKL();
+    }
+    if (raw) {
+        if (p->nacc < 6)
+            CK(cudaMemsetAsync(raw, 0, 6 * (size_t)p->g.tnz * p->g.tnx * sizeof(float), st));
+        raw_out_kernel<<<grid_blocks((long long)p->nacc * p->g.tnz * p->g.tnx), 256, 0, st>>>(p->g, gacc, p->nacc, raw);
+        p->launches++;
+        CKL();
+    }
+    PostArgs pa;
+    pa.g = p->g;
+    pa.nz = G.nz;
+    pa.nx = G.nx;
+    pa.npml = G.npml;
+    pa.r0 = G.mask_row0;
+    pa.r1 = G.mask_row1;
+    pa.c0 = G.mask_col0;
+    pa.c1 = G.mask_col1;
+    pa.energy = p->nacc == 6;
+    pa.param = param;
+    pa.gacc = gacc;
+    pa.mat = at<float>(ws, p->o_mat);
+    pa.fmax_bits = at<int>(ws, p->o_hdr) + 4;
+    pa.out = grad;
+    CK(cudaMemsetAsync(pa.fmax_bits, 0, 3 * sizeof(int), st));
+    long long nm = (long long)G.nz * G.nx;
+    factor_max_kernel<<<grid_blocks(nm), 256, 0, st>>>(pa);
+    p->launches++;
+    CKL();
+    post_kernel<<<grid_blocks(nm), 256, 0, st>>>(pa);
+    p->launches++;
+    CKL();
+    return PYFWI_OK;
+}
+
+int pyfwi_l2_residual(const float *est, const float *obs, float *res, int64_t n, double *misfit, void *stream)
+{
+    if (!est || !obs || !res || !misfit || n < 0) return fail(PYFWI_E_INVALID, "bad argument");
+    if (n == 0) return PYFWI_OK;
+    l2_kernel<<<grid_blocks(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(est, obs, res, n, misfit);
+    CKL();
+    return PYFWI_OK;
+}
+
+int pyfwi_mean2(const float *a, const float *b, float *out, int64_t n, void *stream)
+{
+    if (!a || !b || !out || n < 0) return fail(PYFWI_E_INVALID, "bad argument");
+    if (n == 0) return PYFWI_OK;
+    mean2_kernel<<<grid_blocks(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(a, b, out, n);
+    CKL();
+    return PYFWI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,141 @@
+"""Device engine: a pyfwi_b200 plan, its workspace, and torch-tensor calls
+into libpyfwi_b200.so.
+
+torch provides device memory and the stream; every arithmetic step of the
+propagator path runs in the library's kernels."""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _stream(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def require_cuda(device):
+    device = torch.device(device)
+    if device.type != "cuda" or not torch.cuda.is_available():
+        raise RuntimeError("pyfwi_b200 runs on a CUDA device only (got %s; CUDA available: %s)"
+                           % (device, torch.cuda.is_available()))
+    return device
+
+
+class Plan:
+    """One propagation plan (geometry + options) and its device workspace."""
+
+    def __init__(self, geom, srcx, srcz, opts, device, chp=None):
+        self.device = require_cuda(device)
+        self.lib = N.lib()
+        self.geom = geom
+        self.opts = opts
+        self._srcx = np.ascontiguousarray(srcx, np.int32)
+        self._srcz = np.ascontiguousarray(srcz, np.int32)
+        self._chp = None if chp is None else np.ascontiguousarray(chp, np.int32)
+        if self._chp is not None:
+            opts.nchp = int(self._chp.size)
+            opts.chp = self._chp.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        h = ctypes.c_void_p()
+        N.check(self.lib.pyfwi_plan_create(ctypes.byref(geom), self._srcx.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                           self._srcz.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                           ctypes.byref(opts), ctypes.byref(h)))
+        self.handle = h
+        size = ctypes.c_size_t()
+        N.check(self.lib.pyfwi_workspace_size(h, ctypes.byref(size)))
+        self.ws_bytes = size.value
+        with torch.cuda.device(self.device):
+            self._ws = torch.empty(self.ws_bytes + 256, dtype=torch.uint8, device=self.device)
+        base = self._ws.data_ptr()
+        self.ws = ctypes.c_void_p((base + 255) // 256 * 256)
+        self.nz, self.nx, self.npml = geom.nz, geom.nx, geom.npml
+        self.ns, self.nr, self.nt_ext = geom.ns, geom.nr, geom.nt_ext
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                self.lib.pyfwi_plan_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+    @staticmethod
+    def workspace_bytes(geom, opts, ns_src):
+        """Workspace size a plan with these settings would need."""
+        L = N.lib()
+        srcx = np.zeros(geom.ns, np.int32)
+        srcz = np.zeros(geom.ns, np.int32)
+        h = ctypes.c_void_p()
+        N.check(L.pyfwi_plan_create(ctypes.byref(geom), srcx.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                    srcz.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(opts),
+                                    ctypes.byref(h)))
+        size = ctypes.c_size_t()
+        N.check(L.pyfwi_workspace_size(h, ctypes.byref(size)))
+        L.pyfwi_plan_destroy(h)
+        return size.value
+
+    def launches(self):
+        c = ctypes.c_int64()
+        N.check(self.lib.pyfwi_launch_count(self.handle, ctypes.byref(c)))
+        return c.value
+
+    def set_model(self, vp, vs, rho, damp_x, damp_z):
+        args = [t.to(self.device, torch.float32).contiguous() for t in (vp, vs, rho, damp_x, damp_z)]
+        N.check(self.lib.pyfwi_set_model(self.handle, self.ws, self.ws_bytes, *[_ptr(t) for t in args],
+                                         _stream(self.device)))
+        self._model_keep = args  # alive until the kernels ran
+
+    def forward(self, src_vals, traces=None):
+        """Run all shots; returns traces [5, nt_ext, ns*nr] (float32, device)."""
+        sv = np.ascontiguousarray(src_vals, np.float32).reshape(-1, 4)
+        if traces is None:
+            traces = torch.empty((5, self.nt_ext, self.ns * self.nr), dtype=torch.float32, device=self.device)
+        N.check(self.lib.pyfwi_forward(self.handle, self.ws, self.ws_bytes,
+                                       sv.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(sv.shape[0]),
+                                       _ptr(traces), _stream(self.device)))
+        return traces
+
+    def gradient(self, residual, param, grad=None, raw=None):
+        """residual: list of 5 device tensors [nt_ext, ns*nr] or None.
+        Returns grad [3, nz, nx] (float32, device)."""
+        res = []
+        for r in residual:
+            res.append(None if r is None else r.to(self.device, torch.float32).contiguous())
+        arr = (ctypes.c_void_p * 5)(*[(r.data_ptr() if r is not None else None) for r in res])
+        if grad is None:
+            grad = torch.empty((3, self.nz, self.nx), dtype=torch.float32, device=self.device)
+        N.check(self.lib.pyfwi_gradient(self.handle, self.ws, self.ws_bytes, arr, int(param), _ptr(grad), _ptr(raw),
+                                        _stream(self.device)))
+        self._res_keep = res
+        return grad
+
+
+def mean2(a, b):
+    """(a + b) / 2 on the device (float32)."""
+    a = a.contiguous()
+    b = b.contiguous()
+    out = torch.empty_like(a)
+    N.check(N.lib().pyfwi_mean2(_ptr(a), _ptr(b), _ptr(out), a.numel(), _stream(a.device)))
+    return out
+
+
+def l2_residual(dest, dobs):
+    """L2 misfit of two dicts of device tensors: (rms as a 0-d float64 device
+    tensor, residual dict)."""
+    first = dest[[*dest][0]]
+    dev = require_cuda(first.device)
+    acc = torch.zeros((), dtype=torch.float64, device=dev)
+    res = {}
+    for p in dest:
+        e = dest[p].to(dev, torch.float32).contiguous()
+        o = dobs[p].to(dev, torch.float32).contiguous()
+        r = torch.empty_like(e)
+        N.check(N.lib().pyfwi_l2_residual(_ptr(e), _ptr(o), _ptr(r), e.numel(), _ptr(acc), _stream(dev)))
+        res[p] = r
+    return acc, res

@@ -1,0 +1,148 @@
+"""``FWI``: PyFWI's inversion driver (src/PyFWI/fwi.py:12-282) on the device
+propagator.
+
+Same constructor and ``__call__(m0, method, iter, freqs, n_params, k_0,
+k_end)``; SciPy's conjugate gradient / L-BFGS-B drive ``fprime_single`` as in
+the reference.  Each misfit evaluation runs forward modelling, the L2
+residual and the adjoint gradient on the device; only the model and
+gradient vectors cross to the host for SciPy.  Regularisation terms (TV,
+Tikhonov, prior, parameter relations) and band-limited misfits are not
+provided: asking for them raises."""
+import numpy as np
+import torch
+from scipy.optimize import fmin_cg, fmin_l_bfgs_b
+
+from . import fwi_tools as tools
+from .processing import COMPONENTS, prepare_residual
+from .wave_propagation import WavePropagator
+
+
+class MemoizeJac:
+    """Cache (f, g) of the last point so f and its gradient cost one
+    evaluation."""
+
+    def __init__(self, fun):
+        self.fun = fun
+        self.x = None
+        self.value = self.jac = None
+
+    def _compute(self, x, *args):
+        if self.x is None or not np.array_equal(x, self.x):
+            self.x = np.asarray(x).copy()
+            self.value, self.jac = self.fun(x, *args)
+
+    def __call__(self, x, *args):
+        self._compute(x, *args)
+        return self.value
+
+    def derivative(self, x, *args):
+        self._compute(x, *args)
+        return self.jac
+
+
+class FWI(WavePropagator):
+    def __init__(self, d_obs, inpa, src, rec_loc, model_shape, components, chpr, n_well_rec=0,
+                 param_functions=None):
+        super().__init__(inpa, src, rec_loc, model_shape, n_well_rec=n_well_rec, chpr=chpr, components=components)
+        if param_functions is None:
+            self.dict2vec = tools.vel_dict2vec
+            self.vec2dict = tools.vec2vel_dict
+            self.model_to_dv = lambda a, args: a
+            self.grad_from_dv = lambda a, args, b: a
+            self.param_functions_args = []
+        else:
+            self.dict2vec = param_functions["dict2vec"]
+            self.vec2dict = param_functions["vec2dict"]
+            self.model_to_dv = param_functions["model_to_dv"]
+            self.grad_from_dv = param_functions["grad_from_dv"]
+            self.param_functions_args = param_functions.get("args", [])
+        for key in ("tv", "tikhonov", "prior_model", "param_relation"):
+            if inpa.get(key):
+                raise NotImplementedError("regularisation '%s' is not provided" % key)
+        self.sd = inpa.get("sd", 1.0)
+        if inpa.get("cost_function_type", "l2") != "l2":
+            raise NotImplementedError("only the 'l2' misfit is provided")
+        self.grad_coeff = inpa.get("grad_coeff", [1.0, 1.0, 1.0])
+        self.n_elements = self.nz * self.nx
+        obs = prepare_residual({k: self._to_device(v) for k, v in d_obs.items()}, 1)
+        self.d_obs = {k: v for k, v in obs.items() if bool(torch.any(v != 0))}
+
+    def __call__(self, m0, method, iter, freqs, n_params, k_0, k_end):
+        m = self.dict2vec(m0)
+        method = self._method(method)
+        rms = []
+        k_0 = k_0 - 1
+        k_end -= 1
+        if k_0 + n_params > k_end:
+            raise Exception("k_0 + n_params can't be larger than k_end!!")
+        for c, freq in enumerate(freqs):
+            m, rms0 = method(m, iter[c], freq, n_params, k_0, k_end)
+            rms.append(rms0)
+        return self.vec2dict(m, self.nz, self.nx), np.array(rms, dtype=object)
+
+    def _method(self, user_method):
+        if user_method in [0, "SD", "sd"]:
+            raise NotImplementedError("Steepest descent is not provided yet.")
+        if user_method in [1, "CG", "cg"]:
+            return self.cg
+        if user_method in [2, "lbfgs"]:
+            return self.lbfgs
+        raise ValueError("unknown optimisation method %r" % (user_method,))
+
+    def cg(self, m0, ITER, freq, n_params=1, k0=1, k_end=2):
+        n = self.nz * self.nx
+        mtotal = np.copy(m0)
+        hist = []
+        fun = MemoizeJac(self.fprime_single)
+        for k in np.arange(k0, k_end, n_params):
+            m_1, m_opt, m1 = mtotal[:k * n], mtotal[k * n:(k + n_params) * n], mtotal[(k + n_params) * n:]
+            m_opt, fopt, _, _, _ = fmin_cg(fun, m_opt, fun.derivative, args=(m_1, m1, freq), gtol=1e-8, maxiter=ITER,
+                                          full_output=True, disp=False)
+            hist.append(fopt)
+            mtotal = np.hstack((m_1, m_opt, m1))
+        return mtotal, hist
+
+    def lbfgs(self, m0, ITER, freq, n_params=1, k0=1, k_end=2):
+        n = self.nz * self.nx
+        mtotal = np.copy(m0)
+        hist = []
+        fun = MemoizeJac(self.fprime_single)
+        for k in np.arange(k0, k_end, n_params):
+            m_1, m_opt, m1 = mtotal[:k * n], mtotal[k * n:(k + n_params) * n], mtotal[(k + n_params) * n:]
+            m_opt, fopt, _ = fmin_l_bfgs_b(fun, m_opt, fun.derivative, args=(m_1, m1, freq), m=10, factr=1e7,
+                                           pgtol=1e-8, bounds=None, maxfun=15000, maxiter=ITER, disp=None,
+                                           callback=None, maxls=10)
+            hist.append(fopt)
+            mtotal = np.hstack((m_1, m_opt, m1))
+        return mtotal, hist
+
+    def fprime(self, m0, freq):
+        """Misfit and its gradient (as a vector) at model vector m0."""
+        if freq:
+            raise NotImplementedError("band-limited misfit (freq) is not provided")
+        m_old = self.vec2dict(np.copy(m0), self.nz, self.nx)
+        m_new = self.model_to_dv(m_old, self.param_functions_args)
+        d_est = self.forward_modeling({k: self._to_device(m_new[k]) for k in ("vp", "vs", "rho")}, show=False)
+        d_est = {k: self.sd * v for k, v in d_est.items()}
+        rms = torch.zeros((), dtype=torch.float64, device=self.device)
+        adj = {}
+        for k in COMPONENTS:
+            if k in d_est or k in self.d_obs:
+                est = d_est.get(k, torch.zeros_like(next(iter(d_est.values()))))
+                obs = self.d_obs.get(k, torch.zeros_like(est))
+                r, res = tools.CostFunction("l2")({k: est}, {k: obs})
+                rms += r
+                adj[k] = res[k]
+        grad_dv = self.gradient(adj, parameterization="dv")
+        grad_dv = {k: v.cpu().numpy() for k, v in grad_dv.items()}
+        grad = self.grad_from_dv(grad_dv, self.param_functions_args, m_old)
+        params = [*grad]
+        for q in range(3):
+            grad[params[q]] = grad[params[q]] * self.grad_coeff[q]
+        return float(rms.item()), self.dict2vec(grad)
+
+    def fprime_single(self, m0, m_1, m1, freq):
+        mtotal = np.float32(np.hstack((m_1, m0, m1)))
+        s1, s0 = np.shape(m_1)[0], np.shape(m0)[0]
+        rms, grad = self.fprime(mtotal, freq)
+        return rms, grad[s1:s1 + s0]

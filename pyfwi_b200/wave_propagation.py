@@ -1,0 +1,381 @@
+"""Drop-in ``WavePropagator`` for PyFWI's elastic propagator
+(src/PyFWI/wave_propagation.py).
+
+Same constructor, ``forward_modeling`` and ``gradient`` as the reference and
+the same set-up attributes (nt, nt_ext, dt, dt_scale, tnz, tnx, chp, srcx,
+srcz, dxr, rec_* constants, dx_pml, dz_pml ...).  The per-step OpenCL loop
+of the reference is replaced by one call into libpyfwi_b200.so per
+``forward_modeling`` / ``gradient``; the checkpoints live in device memory.
+
+Inputs may be numpy arrays (outputs are then numpy, as in the reference) or
+torch tensors (outputs stay on the device).
+
+Extra ``inpa`` keys (all optional): ``checkpoint`` ('exact' or 'reverse';
+default: 'exact' when chpr == 100, else the reference's reverse-time scheme),
+``segment`` (steps per recompute segment), ``shot_batch``, ``tile`` (kernel
+variant), ``device``-independent ``cuda_device`` (torch device string).
+"""
+import warnings
+
+import numpy as np
+import torch
+
+from . import _native as N
+from . import acquisition as acq
+from . import fwi_tools as tools
+from .engine import Plan, mean2
+from .processing import COMPONENTS
+
+FIELDS = COMPONENTS
+
+
+def _slice_bounds(start, stop, n):
+    """[lo, hi) of python slice(start, stop) on length n (empty -> (0, 0))."""
+    lo, hi, _ = slice(int(start), int(stop)).indices(int(n))
+    return (lo, hi) if hi > lo else (0, 0)
+
+
+class WavePreparation:
+    """Set-up of a survey (wave_propagation.py:16-246): time-step split, grid
+    padding, index constants, checkpoint schedule and damping arrays, then a
+    device plan for them."""
+
+    def __init__(self, inpa, src, rec_loc, model_shape, components=0, n_well_rec=0, chpr=10):
+        keys = [*inpa]
+        # time axis (wave_propagation.py:28-35)
+        self.dt_scale = np.ceil(inpa["dt"] / 0.0006)
+        self.t = inpa["t"]
+        self.dt_ext = inpa["dt"]
+        self.dt = inpa["dt"] / self.dt_scale
+        self.fn = 1.0 / 2.0 / 0.0006
+        self.nt = int(1 + self.t // self.dt)
+        self.nt_ext = int(1 + self.t // self.dt_ext)
+        self.nx = np.int32(model_shape[1])
+        self.nz = np.int32(model_shape[0])
+        self.seismo_shape = inpa["seimogram_shape"] if "seimogram_shape" in keys else "2d"
+        self.g_smooth = inpa["g_smooth"] if "g_smooth" in keys else 0
+        if "npml" in keys:
+            self.npml, pmlR, pml_dir = inpa["npml"], inpa["pmlR"], inpa["pml_dir"]
+        else:
+            self.npml, pmlR, pml_dir = 0, 0, 2
+        self.sdo = np.int32(inpa["sdo"] / 2) if "sdo" in keys else 2
+        rec_dis = inpa["rec_dis"] if "rec_dis" in keys else (rec_loc[1, :] - rec_loc[0, :]).max()
+        self.acq_type = inpa["acq_type"] if "acq_type" in keys else 1
+        self.energy_balancing = inpa["energy_balancing"] if "energy_balancing" in keys else False
+        self.tnx = np.int32(self.nx + 2 * self.npml)
+        self.tnz = np.int32(self.nz + 2 * self.npml)
+        self.dh = np.float32(inpa["dh"])
+        self.srcx = np.int32(src.i + self.npml)
+        self.srcz = np.int32(src.j + self.npml)
+        self.src = src
+        self.ns = np.int32(src.i.size)
+        self.dxr = np.int32(rec_dis / self.dh)
+        # checkpoint schedule (wave_propagation.py:95-100)
+        nchp = int(chpr * self.nt / 100)
+        self.chp = np.linspace(0, self.nt - 1, nchp, dtype=np.int32)
+        if len(self.chp) < 2:
+            self.chp = np.array([1, self.nt - 1])
+        self.nchp = len(self.chp)
+        self.chpr = chpr
+        self.rec_loc = rec_loc
+        self.nr = rec_loc.shape[0]
+        self.n_well_rec = n_well_rec
+        self.n_surface_rec = self.nr - 2 * n_well_rec
+        if n_well_rec == 0 and self.acq_type == 2:
+            raise Exception(" Number of geophons in the wells is not defined")
+        # receiver index constants (wave_propagation.py:116-144)
+        z = np.int32(0)
+        self.rec_top_left_const = self.rec_top_left_var = z
+        self.rec_top_right_const = self.rec_top_right_var = z
+        self.rec_surface_const = self.rec_surface_var = z
+        if self.acq_type == 0:
+            self.rec_top_right_const = np.int32(rec_loc[0, 0] / self.dh + self.npml)
+            self.rec_top_right_var = np.int32(rec_loc[0, 1] / self.dh + self.npml)
+            self.src_cts = src.i[0]
+        elif self.acq_type == 1:
+            self.rec_surface_const = np.int32(rec_loc[0, 1] / self.dh + self.npml)
+            self.rec_surface_var = np.int32(rec_loc[0, 0] / self.dh + self.npml)
+            self.src_cts = src.j[0]
+        elif self.acq_type == 2:
+            a = np.int32(rec_loc[-self.n_well_rec, :] / self.dh + self.npml)
+            self.rec_top_right_const, self.rec_top_right_var = np.copy(a[0]), np.copy(a[1])
+            a = np.int32(rec_loc[self.n_well_rec, :] / self.dh + self.npml)
+            self.rec_surface_const, self.rec_surface_var = np.copy(a[1]), np.copy(a[0])
+            self.rec_top_left_const = np.int32(rec_loc[0, 0] / self.dh + self.npml)
+            self.rec_top_left_var = np.int32(rec_loc[:, 1] / self.dh + self.npml)[0]
+            self.src_cts = src.j[0]
+        else:
+            raise ValueError("acq_type must be 0, 1 or 2")
+        self.dx_pml, self.dz_pml = tools.pml_counstruction(self.tnz, self.tnx, self.dh, self.npml, pmlR, pml_dir)
+        self.D = tools.Fdm(order=self.sdo * 2)
+        self.components = components
+        self.inpa = dict(inpa)
+        self.device = torch.device(inpa.get("cuda_device", "cuda"))
+        self._wavelet = self._source_values()
+        self._plan = None  # built on first use (device memory is sized then)
+        self._traces = None
+
+    @property
+    def plan(self):
+        if self._plan is None:
+            self._build_plan(self.inpa)
+        return self._plan
+
+    # ---- geometry for the native plan --------------------------------------
+    def _lines(self):
+        """Receiver lines equivalent to the reference's receiver work items
+        (elastic_surface.cl:30-39, elastic_crosswell.cl:95-102,
+        elastic.cl:65-96): cell positions follow the reference's flat index
+        (a column past the last one continues on the next row)."""
+        tnz, tnx, dxr, nr = int(self.tnz), int(self.tnx), int(self.dxr), int(self.nr)
+        if dxr < 1:
+            raise ValueError("receiver spacing rec_dis / dh must be at least 1 cell")
+        groups = []  # (slot0, [(row, col)], vz_from_vx)
+
+        def row_group(row, col0, n_main, slot0):
+            cells = []
+            if 0 <= row < tnz:
+                for j in range(0, tnx, dxr):
+                    ir = j // dxr
+                    if ir >= n_main:
+                        break
+                    flat = row * tnx + j + col0
+                    cells.append(divmod(flat, tnx))
+            return slot0, cells
+
+        def col_group(col, row0, limit, slot0, vzx):
+            cells = []
+            if 0 <= col < tnx:
+                for i in range(0, tnz, dxr):
+                    ir = i // dxr
+                    if ir >= limit or slot0 + ir >= nr:
+                        break
+                    cells.append((i + row0, col))
+            return slot0, cells, vzx
+
+        if self.acq_type == 1:
+            s0, cells = row_group(int(self.rec_surface_const), int(self.rec_surface_var), int(self.n_surface_rec), 0)
+            groups.append((s0, cells, 0))
+        elif self.acq_type == 0:
+            groups.append(col_group(int(self.rec_top_right_const), int(self.rec_top_right_var), nr, 0, 1))
+        else:
+            nw, nm = int(self.n_well_rec), int(self.n_surface_rec)
+            groups.append(col_group(int(self.rec_top_left_const), int(self.rec_top_left_var), nw, 0, 0))
+            s0, cells = row_group(int(self.rec_surface_const), int(self.rec_surface_var), nm, nw)
+            groups.append((s0, cells, 0))
+            groups.append(col_group(int(self.rec_top_right_const), int(self.rec_top_right_var), nr, nw + nm, 0))
+        lines = []
+        for slot0, cells, vzx in groups:
+            # cells outside the grid are read out of bounds by the reference; drop them
+            keep = [(k, rc) for k, rc in enumerate(cells) if 0 <= rc[0] < tnz and 0 <= rc[1] < tnx]
+            if not keep:
+                continue
+            if keep[0][0] != 0 or any(k != q for q, (k, _) in enumerate(keep)):
+                raise NotImplementedError("receiver line leaves the grid in its middle")
+            rows = {rc[0] for _, rc in keep}
+            if len(keep) == 1:
+                lines.append((keep[0][1][0], keep[0][1][1], 0, 1, 1, slot0, vzx))
+            elif len(rows) == 1:
+                step = keep[1][1][1] - keep[0][1][1]
+                if step <= 0 or any(keep[q][1][1] - keep[q - 1][1][1] != step for q in range(1, len(keep))):
+                    raise NotImplementedError("surface receiver line wraps to the next grid row")
+                lines.append((keep[0][1][0], keep[0][1][1], 0, step, len(keep), slot0, vzx))
+            else:
+                step = keep[1][1][0] - keep[0][1][0]
+                lines.append((keep[0][1][0], keep[0][1][1], step, 0, len(keep), slot0, vzx))
+        if not lines:
+            lines.append((0, 0, 0, 1, 0, 0, 0))
+        return lines
+
+    def _mask_window(self):
+        sdo, nz, nx = int(self.sdo), int(self.nz), int(self.nx)
+        cts = int(self.src_cts)
+        if self.acq_type == 0:
+            r = _slice_bounds(sdo, -sdo, nz)
+            c = _slice_bounds(sdo + cts + 2, -sdo, nx)
+        else:
+            r = _slice_bounds(sdo + cts + 2, -sdo, nz)
+            c = _slice_bounds(sdo, -sdo, nx)
+        return r + c
+
+    def _geometry(self):
+        g = N.Geometry()
+        g.nz, g.nx, g.npml = int(self.nz), int(self.nx), int(self.npml)
+        g.half_order = int(self.sdo)
+        g.nt, g.nt_ext, g.dt_scale = int(self.nt), int(self.nt_ext), int(self.dt_scale)
+        # the reference bakes dt, dh and c1..c4 into its kernels through "%f"
+        # (wave_propagation.py:434-490)
+        r6 = lambda x: float("%f" % x)
+        g.dt = r6(self.dt)
+        g.dh = r6(self.dh)
+        for q, c in enumerate((self.D.c1, self.D.c2, self.D.c3, self.D.c4)):
+            g.c[q] = r6(c)
+        g.ns, g.nr = int(self.ns), int(self.nr)
+        lines = self._lines()
+        g.n_lines = len(lines)
+        for q, (r0, c0, dr, dc, cnt, s0, vzx) in enumerate(lines):
+            g.lines[q] = N.RecLine(r0, c0, dr, dc, cnt, s0, vzx)
+        g.mask_row0, g.mask_row1, g.mask_col0, g.mask_col1 = self._mask_window()
+        return g
+
+    def _source_values(self):
+        """(vx, vz, taux, tauz) amplitudes for each injection
+        (wave_propagation.py:652-664)."""
+        n_inj = int(np.ceil(self.nt / self.dt_scale))
+        vals = np.zeros((n_inj, 4), np.float32)
+        for k in range(n_inj):
+            vals[k] = np.float32(self.src(k))[:4]
+        return vals
+
+    def _build_plan(self, inpa):
+        mode = inpa.get("checkpoint", "exact" if self.chpr == 100 else "reverse")
+        if mode not in ("exact", "reverse"):
+            raise ValueError("inpa['checkpoint'] must be 'exact' or 'reverse'")
+        self.checkpoint = mode
+        geom = self._geometry()
+        srcx = np.asarray(self.srcx, np.int32).reshape(-1)
+        srcz = np.asarray(self.srcz, np.int32).reshape(-1)
+        chp = np.asarray(self.chp, np.int32) if mode == "reverse" else None
+
+        def opts(seg, batch):
+            o = N.Options()
+            o.checkpoint = N.CKPT_EXACT if mode == "exact" else N.CKPT_REVERSE
+            o.segment = int(seg)
+            o.snapshot = N.SNAP_FP32
+            o.shot_batch = int(batch)
+            o.energy = 1 if self.energy_balancing else 0
+            o.tile = int(inpa.get("tile", 0))
+            o.graph = 0
+            if chp is not None:
+                o.nchp = int(chp.size)
+                o.chp = chp.ctypes.data_as(N.ctypes.POINTER(N.ctypes.c_int32))
+            return o
+
+        seg = int(inpa.get("segment", 0))
+        batch = int(inpa.get("shot_batch", 0))
+        if mode == "exact" and ("segment" not in inpa or "shot_batch" not in inpa):
+            seg, batch = self._auto_layout(geom, opts, seg, batch)
+        self._plan = Plan(geom, srcx, srcz, opts(seg, batch), self.device, chp=chp)
+        self.segment, self.shot_batch = seg, batch
+
+    def _auto_layout(self, geom, opts, seg, batch):
+        """Largest segment (fewest recomputed steps) and shot batch whose
+        workspace fits in free device memory."""
+        free, _ = torch.cuda.mem_get_info(self.device)
+        traces = 5 * self.nt_ext * int(self.ns) * int(self.nr) * 4
+        budget = int(0.9 * free) - 4 * traces - (256 << 20)
+        nt, ns = int(self.nt), int(self.ns)
+        batches = [batch] if batch else sorted({ns, (ns + 1) // 2, (ns + 3) // 4, 1}, reverse=True)
+        for b in batches:
+            k = 1
+            while True:
+                s = seg or -(-nt // k)
+                if Plan.workspace_bytes(geom, opts(s, b), ns) <= budget:
+                    return s, b
+                if seg or s * s < nt:
+                    break
+                k += 1
+        raise MemoryError("the survey does not fit in device memory (%.1f GB free)" % (free / 2 ** 30))
+
+    # ---- helpers ---------------------------------------------------------
+    def _to_device(self, x):
+        if isinstance(x, torch.Tensor):
+            return x.to(self.device, torch.float32)
+        return torch.from_numpy(np.ascontiguousarray(x, np.float32)).to(self.device, non_blocking=False)
+
+
+class WavePropagator(WavePreparation):
+    """Forward modelling and adjoint-state gradient (wave_propagation.py:594-938).
+
+    Parameters as the reference: ``inpa`` dict, ``src`` (acquisition.Source
+    with a wavelet), ``rec_loc`` (nr, 2) in metres, ``model_shape``,
+    ``components`` (0: (taux+tauz)/2, 1: taux, 2: vx vz, 3: stresses, 4: all),
+    ``n_well_rec``, ``chpr`` (checkpoint percentage)."""
+
+    def __init__(self, inpa, src, rec_loc, model_shape, components=0, n_well_rec=0, chpr=0):
+        WavePreparation.__init__(self, inpa=inpa, src=src, rec_loc=rec_loc, model_shape=model_shape,
+                                 components=components, n_well_rec=n_well_rec, chpr=chpr)
+
+    # ------------------------------------------------------------------
+    def forward_modeling(self, model0, show=False):
+        """Seismic section of the model dict {'vp', 'vs', 'rho'} ((nz, nx)
+        arrays or tensors) in the shape set by inpa['seimogram_shape']."""
+        if show:
+            warnings.warn("show=True: live wavefield plotting is not available; ignored")
+        as_numpy = not isinstance(model0["vp"], torch.Tensor)
+        vp, vs, rho = (self._to_device(model0[k]) for k in ("vp", "vs", "rho"))
+        damp_x = torch.from_numpy(np.ascontiguousarray(self.dx_pml[0, :]))
+        damp_z = torch.from_numpy(np.ascontiguousarray(self.dz_pml[:, 0]))
+        self.plan.set_model(vp, vs, rho, damp_x, damp_z)
+        self._traces = self.plan.forward(self._wavelet, self._traces)
+        self._model_dev = (vp, vs, rho)
+        data = self._section(self._traces)
+        if as_numpy:
+            data = {k: v.cpu().numpy() for k, v in data.items()}
+        return data
+
+    def _section(self, traces):
+        """acquisition.seismic_section on device traces [5][nt_ext][ns*nr]."""
+        nt, ns, nr = int(self.nt_ext), int(self.ns), int(self.nr)
+        tr = traces
+        if self.acq_type == 2 and self.n_well_rec:
+            # wave_propagation.py:647-649: the left-well traces come out in reverse order
+            nw = int(self.n_well_rec)
+            idx = torch.arange(ns * nr, device=self.device).view(ns, nr)
+            idx[:, :nw] = idx[:, :nw].flip(1)
+            tr = traces.index_select(2, idx.reshape(-1))
+        comp = {k: tr[q] for q, k in enumerate(FIELDS)}
+        if self.components == 0:
+            m = mean2(comp["taux"], comp["tauz"])
+            data = {"taux": m, "tauz": mean2(comp["taux"], comp["tauz"])}
+        else:
+            data = {k: comp[k] for k in acq.section_keys(self.components)}
+        if self.seismo_shape == "2d":
+            return data
+        return {k: v.view(nt, ns, nr).permute(0, 2, 1) for k, v in data.items()}
+
+    @property
+    def seismogram(self):
+        """Raw receiver traces of the last forward call, (nt_ext, nr, ns) per
+        component (host copies)."""
+        if self._traces is None:
+            return None
+        nt, ns, nr = int(self.nt_ext), int(self.ns), int(self.nr)
+        return {k: self._traces[q].view(nt, ns, nr).permute(0, 2, 1).cpu().numpy() for q, k in enumerate(FIELDS)}
+
+    # ------------------------------------------------------------------
+    def gradient(self, res, show=False, parameterization="dv"):
+        """Gradient of the misfit whose adjoint source is ``res`` (a dict of
+        (nt_ext, nr*ns) arrays or tensors; missing components are zero).
+        Returns {'vp','vs','rho'} ('dv') or {'lam','mu','rho'}."""
+        if show:
+            warnings.warn("show=True: live wavefield plotting is not available; ignored")
+        if self.g_smooth:
+            raise NotImplementedError("gradient smoothing (g_smooth > 0) is not provided")
+        as_numpy = not isinstance(res[[*res][0]], torch.Tensor)
+        nt, nrs = int(self.nt_ext), int(self.nr) * int(self.ns)
+        planes = []
+        for k in FIELDS:
+            if k not in res:
+                planes.append(None)
+                continue
+            r = res[k]
+            if r.ndim == 3:  # (nt, nr, ns) -> (nt, ns*nr)
+                r = (np.transpose(r, (0, 2, 1)) if isinstance(r, np.ndarray) else r.permute(0, 2, 1))
+            r = self._to_device(r).reshape(nt, nrs).contiguous()
+            planes.append(r)
+        param = N.PARAM_DV if parameterization == "dv" else N.PARAM_LMD
+        g = self.plan.gradient(planes, param)
+        names = ("vp", "vs", "rho") if parameterization == "dv" else ("lam", "mu", "rho")
+        out = {n: g[q] for q, n in enumerate(names)}
+        if as_numpy:
+            out = {k: v.cpu().numpy() for k, v in out.items()}
+        return out
+
+    def raw_gradient(self, res):
+        """The six (tnz, tnx) accumulators (Gmu, Glam, Grho and the energy
+        terms) before masking, for inspection and tests."""
+        planes = [None if k not in res else self._to_device(res[k]).contiguous() for k in FIELDS]
+        raw = torch.zeros((6, int(self.tnz), int(self.tnx)), dtype=torch.float32, device=self.device)
+        self.plan.gradient(planes, N.PARAM_LMD, raw=raw)
+        return raw

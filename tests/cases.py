@@ -166,11 +166,68 @@ def tiny_both():
 
 
 TINY = [tiny_s8, tiny_dtscale, tiny_chpr, tiny_crosswell, tiny_dxr, tiny_both]
-ALL = [c1] + TINY
+ALL = [c1] + TINY  # cases with golden fixtures
 
 
 def by_name(name):
-    for f in ALL:
-        if f.__name__ == name:
-            return f()
-    raise KeyError(name)
+    f = globals().get(name)
+    if f is None or not callable(f) or not (name.startswith("c") or name.startswith("tiny_")):
+        raise KeyError(name)
+    return f()
+
+
+def c2():
+    """200 x 400 cells, dh = 5 m, 20-cell layer; two layers (vp 2000 / 3000,
+    vs = vp / 1.8, Gardner rho = 310 vp^0.25) plus a Gaussian-smoothed random
+    perturbation (3 % std, 10-cell correlation, seeded); 10 Ricker shots at
+    10 Hz, 400 receivers, dt = 0.5 ms, nt = 2000; taux/tauz recorded."""
+    from scipy.ndimage import gaussian_filter
+    nz, nx, dh, dt = 200, 400, 5.0, 0.0005
+    inpa = {"dt": dt, "t": _t_for(2000, dt), "dh": dh, "npml": 20, "pmlR": 1e-5, "pml_dir": 2, "sdo": 4,
+            "rec_dis": dh, "acq_type": 1}
+    vp = np.where(np.arange(nz)[:, None] < nz // 2, 2000.0, 3000.0) + 0 * np.arange(nx)[None, :]
+    rng = np.random.default_rng(2024)
+    pert = gaussian_filter(rng.standard_normal((nz, nx)), 10.0)
+    pert *= 0.03 / pert.std()
+    vp_obs = (vp * (1 + pert)).astype(np.float32)
+    vp_est = gaussian_filter(vp, 5.0).astype(np.float32)
+
+    def mk(v):
+        return {"vp": v, "vs": (v / 1.8).astype(np.float32), "rho": (310 * v ** 0.25).astype(np.float32)}
+
+    ns = 10
+    src_loc = np.stack([np.linspace(20, nx - 21, ns).astype(np.int32) * dh, np.full(ns, 2 * dh)], 1).astype(np.float32)
+    rec_loc = np.stack([np.arange(nx) * dh, np.full(nx, 2 * dh)], 1).astype(np.float32)
+    return dict(name="c2", inpa=inpa, src_loc=src_loc, rec_loc=rec_loc, fdom=10.0, src_type=0, components=0,
+                chpr=100, n_well_rec=0, param="dv", model_obs=mk(vp_obs), model_est=mk(vp_est))
+
+
+def c3(ns=64):
+    """500 x 1000 cells, dh = 5 m, 30-cell layer; vp rising 1800 -> 4000 m/s
+    with depth, three dipping interfaces and a seeded lens (vs = vp / 1.8,
+    Gardner rho); 64 shots at 8 Hz on a 15-cell pitch, 1000 receivers,
+    dt = 0.5 ms, nt = 4000; every step available to the adjoint."""
+    nz, nx, dh, dt = 500, 1000, 5.0, 0.0005
+    inpa = {"dt": dt, "t": _t_for(4000, dt), "dh": dh, "npml": 30, "pmlR": 1e-5, "pml_dir": 2, "sdo": 4,
+            "rec_dis": dh, "acq_type": 1}
+    z = np.arange(nz)[:, None].astype(np.float64)
+    x = np.arange(nx)[None, :].astype(np.float64)
+    vp = 1800.0 + 2000.0 * z / (nz - 1) + 0 * x
+    for k, (z0, slope, jump) in enumerate([(120, 0.08, 120.0), (260, -0.05, 150.0), (380, 0.03, -100.0)]):
+        vp = vp + jump * (z > z0 + slope * (x - nx / 2))
+    rng = np.random.default_rng(33)
+    cz, cx = rng.uniform(180, 320), rng.uniform(350, 650)
+    a, b = rng.uniform(30, 50), rng.uniform(80, 140)
+    lens = ((z - cz) / a) ** 2 + ((x - cx) / b) ** 2 < 1
+    vp = np.where(lens, vp * 0.92, vp)
+    vp = np.clip(vp, 1800.0, 4000.0).astype(np.float32)
+    model = {"vp": vp, "vs": (vp / 1.8).astype(np.float32), "rho": (310 * vp ** 0.25).astype(np.float32)}
+    src_loc = np.stack([(20 + 15 * np.arange(ns)) * dh, np.full(ns, 2 * dh)], 1).astype(np.float32)
+    rec_loc = np.stack([np.arange(nx) * dh, np.full(nx, 2 * dh)], 1).astype(np.float32)
+    smooth = {k: v.copy() for k, v in model.items()}
+    from scipy.ndimage import gaussian_filter
+    smooth["vp"] = gaussian_filter(vp, 8.0).astype(np.float32)
+    smooth["vs"] = (smooth["vp"] / 1.8).astype(np.float32)
+    smooth["rho"] = (310 * smooth["vp"] ** 0.25).astype(np.float32)
+    return dict(name="c3", inpa=inpa, src_loc=src_loc, rec_loc=rec_loc, fdom=8.0, src_type=0, components=0,
+                chpr=100, n_well_rec=0, param="dv", model_obs=model, model_est=smooth)

@@ -24,3 +24,22 @@ def oracle_run(case, precision="fp32", d_obs=None, gradient=True):
         res = {k: (pe[k] - po[k]).astype(W.real) for k in O.FIELDS}
         grad = W.gradient(res, parameterization=case["param"])
     return d_obs, d_est, grad, W
+
+
+def product(case, **extra):
+    """The product's WavePropagator for a case (extra inpa keys allowed)."""
+    from pyfwi_b200 import acquisition as acq
+    from pyfwi_b200.wave_propagation import WavePropagator
+    inpa = dict(case["inpa"])
+    inpa.update(extra)
+    src = acq.Source(case["src_loc"], inpa["dh"], inpa["dt"], case["src_type"])
+    src.Ricker(case["fdom"])
+    return WavePropagator(inpa, src, case["rec_loc"], case["model_est"]["vp"].shape, components=case["components"],
+                          n_well_rec=case["n_well_rec"], chpr=case["chpr"])
+
+
+def l2_residual_np(d_est, d_obs):
+    """CostFunction('l2') of the reference on prepared dicts: float32(est - obs)."""
+    import oracle as O
+    pe, po = O.prepare_residual(d_est, 1), O.prepare_residual(d_obs, 1)
+    return {k: np.float32(pe[k] - po[k]) for k in O.FIELDS}
