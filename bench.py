@@ -1,0 +1,367 @@
+"""Benchmark: FWI gradient evaluations of the 500 x 1000-cell, 64-shot,
+4000-step elastic survey on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one misfit-and-gradient evaluation of all shots: forward
+modelling, L2 residual against the observed data, adjoint-state gradient
+(and, for N > 1, the NCCL sum of the gradient over ranks).  Throughput is
+grid-cell updates per second: padded cells x internal time steps x shots,
+counted once for the forward and once for the adjoint pass.
+
+With N GPUs every rank evaluates its own 64-shot survey (weak scaling) and
+the per-rank gradients are summed with one all-reduce per step.  Rank 0
+prints one JSON line.
+
+--impl reference times the reference's own kernels (PyFWI's elastic.cl /
+elastic_surface.cl compiled for the host CPU; oracle/ref_driver.py) in the
+reference's loop order on a bounded sample of the same survey, with every
+host thread.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (ROOT, os.path.join(ROOT, "tests"), os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "FWI grad Gcell-updates/s & %HBM roofline, batched vs plain per-shot, grad err≤1e-4"
+UNIT = "Gcell-updates/s"
+WORKLOAD = "elastic FWI gradient, 500x1000 cells (+30-cell absorbing layer), 64 shots, 1000 receivers, nt=4000"
+
+# algorithmic bytes per cell and shot-step (one FP32 read or write = 4 B)
+BYTES_FWD = 52.0         # read vx vz txx tzz txz lam mu b, write 5 fields
+BYTES_ADJ = 52.0         # adjoint propagation: same count
+BYTES_IMG = 44.0         # imaging: read 5 forward fields, read+write 3 gradients
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in self.rows for q in range(4) if r[3 + q].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def survey(ns, nt=None):
+    """The 500 x 1000-cell survey with ns shots; nt < 4000 shortens the
+    record (small profiling cases only)."""
+    import cases
+    case = cases.c3(ns=ns)
+    if nt:
+        dt = case["inpa"]["dt"]
+        case["inpa"]["t"] = (nt - 1) * dt + dt / 2
+    return case
+
+
+# --------------------------------------------------------------------------
+# the reference arm and the CPU baseline
+# --------------------------------------------------------------------------
+def cpu_sample(case, seconds=15.0, max_steps=4000):
+    """Time the reference's kernels (or the oracle port when they are not
+    built) on one shot over the first n steps, forward + backward; n is sized
+    for about `seconds` of work.  Returns (Gcell-updates/s, description)."""
+    import oracle as O
+    import ref_driver
+    inpa = case["inpa"]
+    src = O.Ricker(case["src_loc"], inpa["dh"], inpa["dt"], case["src_type"])
+    src.Ricker(case["fdom"])
+    W = O.OracleWavePropagator(inpa, src, case["rec_loc"], case["model_est"]["vp"].shape,
+                               components=case["components"], chpr=0)
+    W._materials(case["model_est"])
+    cells = int(W.tnz) * int(W.tnx)
+    threads = len(os.sched_getaffinity(0))
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    if ref_driver.available(case["name"]):
+        R = ref_driver.RefRunner(case["name"], W)
+        probe = 16
+        t = R.run_shot(0, probe)
+        n = int(min(max_steps, max(probe, seconds / (t / probe))))
+        t = R.run_shot(0, n)
+        kind = "reference"
+        desc = ("PyFWI elastic.cl/elastic_surface.cl compiled for the host (OpenMP, %d threads), reference loop "
+                "order, 1 shot x first %d of %d steps, forward + backward, every step stored" % (threads, n, W.nt))
+    else:
+        import ctypes
+        L = O.lib("fp32")
+        probe = 16
+
+        def run(n):
+            cfg = O.OrcCfg.from_buffer_copy(W.cfg)
+            cfg.nt = n
+            seis = np.zeros((5, W.nt_ext, W.nr), np.float32)
+            store = np.zeros((n, 5, cells), np.float32)
+            chp = np.arange(n, dtype=np.int32)
+            G = [np.zeros(cells, np.float32) for _ in range(6)]
+            res = (ctypes.c_void_p * 5)()
+            t0 = time.perf_counter()
+            L.orc_forward_shot(ctypes.byref(cfg), *W._mats(), int(W.srcx[0]), int(W.srcz[0]), O._ptr(W.src_vals),
+                               W.n_inj, O._ptr(seis), O._ptr(store), O._ptr(chp), n)
+            L.orc_gradient_shot(ctypes.byref(cfg), *W._mats(), res, O._ptr(store), O._ptr(chp), n,
+                                *[O._ptr(g) for g in G])
+            return time.perf_counter() - t0
+
+        t = run(probe)
+        n = int(min(max_steps, max(probe, seconds / (t / probe))))
+        t = run(n)
+        kind = "port"
+        desc = ("oracle restatement (C, OpenMP, %d threads), 1 shot x first %d of %d steps, forward + backward"
+                % (threads, n, W.nt))
+    return 2.0 * cells * n / t / 1e9, kind, threads, desc
+
+
+def run_reference(args, world, rank):
+    case = survey(1)
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        cpu_sample(case, seconds=args.cpu_seconds / 3)
+    vals = []
+    for _ in range(args.steps):
+        v, kind, cores, desc = cpu_sample(case, seconds=args.cpu_seconds)
+        vals.append(v)
+    value = statistics.median(vals)
+    cells = 2.0 * 560 * 1060 * 4000 * 64
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": cells / (value * 1e9) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": desc},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+def run_ours(args, world, rank, local):
+    import torch
+    import torch.distributed as dist
+    from helpers import product
+    from pyfwi_b200 import fwi_tools
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    case = survey(args.shots, args.nt)
+    extra = {"cuda_device": str(dev)}
+    if args.segment:
+        extra.update(segment=args.segment, shot_batch=args.shots)
+    if args.tile is not None:
+        extra["tile"] = args.tile
+    W = product(case, **extra)
+    ncell = float(int(W.tnz) * int(W.tnx))
+    nint = float((int(W.tnz) - 2 * (int(W.npml) + int(W.sdo)) + 1) * (int(W.tnx) - 2 * (int(W.npml) + int(W.sdo)) + 1))
+    cell_updates = 2.0 * ncell * int(W.nt) * int(W.ns)  # forward + adjoint
+
+    m_est = {k: torch.from_numpy(v).to(dev) for k, v in case["model_est"].items()}
+    m_obs = {k: torch.from_numpy(v).to(dev) for k, v in case["model_obs"].items()}
+    d_obs = {k: v.clone() for k, v in W.forward_modeling(m_obs).items()}
+
+    def allreduce(grad, rms):
+        if world > 1:
+            dist.all_reduce(grad)
+            dist.all_reduce(rms)
+
+    def step(model, obs):
+        d_est = W.forward_modeling(model)
+        rms, res = fwi_tools.CostFunction("l2")(d_est, obs)
+        grad = W.gradient(res, parameterization="dv")
+        g = torch.stack([grad["vp"], grad["vs"], grad["rho"]])
+        allreduce(g, rms)
+        return g, rms
+
+    for _ in range(args.warmup):
+        step(m_est, d_obs)
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local) if rank == 0 else None
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    W.plan.profile(True)
+    launches0 = W.plan.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        g, rms = step(m_est, d_obs)
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = W.plan.launches() - launches0
+    clocks = sampler.stop() if sampler else None
+    W.plan.profile(False)
+    prof = {k: W.plan.profile_read(k) for k in (0, 1, 2)}
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * cell_updates * args.steps / (ms_max * 1e-3) / 1e9
+
+    # end to end through the public API from pinned host buffers
+    host_model = {k: v.cpu().pin_memory() for k, v in m_est.items()}
+    host_obs = {k: v.cpu().pin_memory() for k, v in d_obs.items()}
+    h2d = sum(v.numel() * 4 for v in host_model.values()) + sum(v.numel() * 4 for v in host_obs.values())
+    out_host = torch.empty((3, int(W.nz), int(W.nx)), dtype=torch.float32).pin_memory()
+    rms_host = torch.empty((), dtype=torch.float64).pin_memory()
+    d2h = out_host.numel() * 4 + 8
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record()
+    for _ in range(args.steps):
+        model = {k: v.to(dev, non_blocking=True) for k, v in host_model.items()}
+        obs = {k: v.to(dev, non_blocking=True) for k, v in host_obs.items()}
+        g, rms = step(model, obs)
+        out_host.copy_(g, non_blocking=True)
+        rms_host.copy_(rms, non_blocking=True)
+    e3.record()
+    torch.cuda.synchronize()
+    t = torch.tensor([e2.elapsed_time(e3)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * cell_updates * args.steps / (float(t.item()) * 1e-3) / 1e9
+
+    if rank != 0:
+        return
+    hbm, peak_src = peaks()
+    # dominant kernel: the one with the most device time
+    kinds = {0: ("fwd_step", BYTES_FWD), 1: ("adj_step", None), 2: ("rev_step", BYTES_FWD)}
+    dom = max(prof, key=lambda k: prof[k][1])
+    n_l, ms_k, cells_k = prof[dom]
+    name, bpc = kinds[dom]
+    if dom == 1:
+        alg_bytes = cells_k * BYTES_ADJ + (cells_k / ncell) * nint * BYTES_IMG
+    else:
+        alg_bytes = cells_k * bpc
+    achieved = alg_bytes / (ms_k * 1e-3) / 1e9 if ms_k > 0 else None
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic_%s_c3.json" % name)
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tj = json.load(f)
+        traffic = tj["dram_bytes_per_cell_shot"] * cells_k / max(n_l, 1)
+    roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm if achieved else None, "traffic": traffic, "peak_source": peak_src,
+            "launches": n_l, "avg_launch_ms": ms_k / max(n_l, 1),
+            "alg_bytes_per_launch": alg_bytes / max(n_l, 1),
+            "kernel_share": {kinds[k][0]: prof[k][1] / max(ms, 1e-9) for k in prof}}
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        v, kind, cores, desc = cpu_sample(survey(1), seconds=args.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "shots_per_gpu": int(W.ns), "nt": int(W.nt),
+                       "grid": [int(W.tnz), int(W.tnx)], "checkpoint": W.checkpoint, "segment": W.segment,
+                       "shot_batch": W.shot_batch, "parallelism": "dp%d" % world,
+                       "l2": "inputs larger than L2 (no flush)"},
+            "roofline": roof, "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches, "clocks": clocks,
+            "misfit": float(rms.item())}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--shots", type=int, default=64)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--nt", type=int, default=None, help="shorter record (profiling cases)")
+    ap.add_argument("--segment", type=int, default=0, help="steps per recompute segment (default: auto)")
+    ap.add_argument("--tile", type=int, default=None, help="kernel tile variant")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        # rank 0 alone times the host CPU; other ranks have nothing to do
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        run_reference(args, world, int(os.environ.get("RANK", "0")))
+        return
+    world, rank, local = dist_setup(args)
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

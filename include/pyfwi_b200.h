@@ -155,6 +155,15 @@ int pyfwi_l2_residual(const float *est, const float *obs, float *res, int64_t n,
 /* Trace section (acquisition.py:313-333): out = (a + b) / 2 elementwise. */
 int pyfwi_mean2(const float *a, const float *b, float *out, int64_t n, void *stream);
 
+/* Per-kernel timing.  While enabled, every step kernel the plan launches is
+ * bracketed by CUDA events on the caller's stream.  pyfwi_profile_read
+ * synchronises on those events and returns, for one kernel kind (0 forward
+ * step, 1 adjoint+imaging step, 2 reverse step), the launches, the summed
+ * device milliseconds and the summed grid cells x shots they processed; it
+ * then clears the counters. */
+int pyfwi_profile_enable(pyfwi_plan *plan, int32_t enable);
+int pyfwi_profile_read(pyfwi_plan *plan, int32_t kind, int64_t *launches, double *ms, double *cell_shots);
+
 /* Number of kernel tile variants the autotuner may choose between. */
 int pyfwi_tile_count(int32_t half_order);
 

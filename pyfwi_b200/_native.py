@@ -61,11 +61,14 @@ def lib():
     L.pyfwi_mean2.argtypes = [_P, _P, _P, ctypes.c_int64, _P]
     L.pyfwi_tile_count.argtypes = [_i32]
     L.pyfwi_launch_count.argtypes = [_P, ctypes.POINTER(ctypes.c_int64)]
+    L.pyfwi_profile_enable.argtypes = [_P, _i32]
+    L.pyfwi_profile_read.argtypes = [_P, _i32, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(ctypes.c_double)]
     L.pyfwi_last_error.restype = ctypes.c_char_p
     L.pyfwi_abi_version.restype = ctypes.c_int
     for name in ("pyfwi_plan_create", "pyfwi_plan_destroy", "pyfwi_workspace_size", "pyfwi_set_model",
                  "pyfwi_forward", "pyfwi_gradient", "pyfwi_l2_residual", "pyfwi_mean2", "pyfwi_tile_count",
-                 "pyfwi_launch_count"):
+                 "pyfwi_launch_count", "pyfwi_profile_enable", "pyfwi_profile_read"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -66,6 +66,17 @@ struct pyfwi_plan {
     size_t o_hdr, o_src, o_mat, o_dampx, o_dampz, o_work, o_adj, o_gacc, o_store, o_store16, total;
     long long launches = 0;
     bool model_set = false, fwd_valid = false;
+    // per-kernel event timing (pyfwi_profile_enable)
+    bool profiling = false;
+    struct Ev {
+        cudaEvent_t a, b;
+        int kind;
+        double cells;
+    };
+    std::vector<Ev> events;
+    size_t ev_used = 0;
+    double prof_ms[3] = {0, 0, 0}, prof_cells[3] = {0, 0, 0};
+    long long prof_n[3] = {0, 0, 0};
     void *ws_initialised = nullptr;
 };
 
@@ -134,8 +145,33 @@ int launch_adj(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
     return p->nacc == 6 ? launch_adj_t<R, TZ, true>(p, a, nslots, s) : launch_adj_t<R, TZ, false>(p, a, nslots, s);
 }
 
+// Event pair around one step launch when profiling (kind 0 fwd, 1 adj, 2 rev).
+struct ProfileScope {
+    pyfwi_plan *p;
+    cudaStream_t s;
+    pyfwi_plan::Ev *ev = nullptr;
+    ProfileScope(pyfwi_plan *p_, cudaStream_t s_, int kind, int nslots) : p(p_), s(s_)
+    {
+        if (!p->profiling) return;
+        if (p->ev_used == p->events.size()) {
+            pyfwi_plan::Ev e{};
+            if (cudaEventCreate(&e.a) != cudaSuccess || cudaEventCreate(&e.b) != cudaSuccess) return;
+            p->events.push_back(e);
+        }
+        ev = &p->events[p->ev_used++];
+        ev->kind = kind;
+        ev->cells = (double)p->g.tnz * p->g.tnx * nslots;
+        cudaEventRecord(ev->a, s);
+    }
+    ~ProfileScope()
+    {
+        if (ev) cudaEventRecord(ev->b, s);
+    }
+};
+
 int step_fwd(pyfwi_plan *p, const StepArgs &a, int nslots, cudaStream_t s, bool reverse)
 {
+    ProfileScope prof(p, s, reverse ? 2 : 0, nslots);
 #define CASE(R_, TZ_) \
     if (p->R == R_ && p->tz == TZ_) return launch_fwd<R_, TZ_>(p, a, nslots, s, reverse);
     CASE(2, 16) CASE(2, 8) CASE(2, 32) CASE(4, 16) CASE(4, 8) CASE(4, 32)
@@ -145,6 +181,7 @@ int step_fwd(pyfwi_plan *p, const StepArgs &a, int nslots, cudaStream_t s, bool 
 
 int step_adj(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
 {
+    ProfileScope prof(p, s, 1, nslots);
 #define CASE(R_, TZ_) \
     if (p->R == R_ && p->tz == TZ_) return launch_adj<R_, TZ_>(p, a, nslots, s);
     CASE(2, 16) CASE(2, 8) CASE(2, 32) CASE(4, 16) CASE(4, 8) CASE(4, 32)
@@ -431,7 +468,43 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
 
 int pyfwi_plan_destroy(pyfwi_plan *plan)
 {
+    if (plan)
+        for (auto &e : plan->events) {
+            cudaEventDestroy(e.a);
+            cudaEventDestroy(e.b);
+        }
     delete plan;
+    return PYFWI_OK;
+}
+
+int pyfwi_profile_enable(pyfwi_plan *p, int32_t enable)
+{
+    if (!p) return fail(PYFWI_E_INVALID, "NULL plan");
+    p->profiling = enable != 0;
+    return PYFWI_OK;
+}
+
+int pyfwi_profile_read(pyfwi_plan *p, int32_t kind, int64_t *launches, double *ms, double *cells)
+{
+    if (!p || !launches || !ms || !cells) return fail(PYFWI_E_INVALID, "NULL argument");
+    if (kind < 0 || kind > 2) return fail(PYFWI_E_INVALID, "kind must be 0, 1 or 2");
+    // fold every pending event pair into the per-kind totals
+    for (size_t q = 0; q < p->ev_used; ++q) {
+        auto &e = p->events[q];
+        CK(cudaEventSynchronize(e.b));
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, e.a, e.b));
+        p->prof_n[e.kind] += 1;
+        p->prof_ms[e.kind] += t;
+        p->prof_cells[e.kind] += e.cells;
+    }
+    p->ev_used = 0;
+    *launches = p->prof_n[kind];
+    *ms = p->prof_ms[kind];
+    *cells = p->prof_cells[kind];
+    p->prof_n[kind] = 0;
+    p->prof_ms[kind] = 0.0;
+    p->prof_cells[kind] = 0.0;
     return PYFWI_OK;
 }
 

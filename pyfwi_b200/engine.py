@@ -85,6 +85,18 @@ class Plan:
         N.check(self.lib.pyfwi_launch_count(self.handle, ctypes.byref(c)))
         return c.value
 
+    def profile(self, enable=True):
+        """Bracket every step kernel with CUDA events (see profile_read)."""
+        N.check(self.lib.pyfwi_profile_enable(self.handle, 1 if enable else 0))
+
+    def profile_read(self, kind):
+        """(launches, device ms, grid cells x shots) of kind 0 forward step,
+        1 adjoint+imaging step, 2 reverse step since the last read."""
+        n, ms, cells = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+        N.check(self.lib.pyfwi_profile_read(self.handle, int(kind), ctypes.byref(n), ctypes.byref(ms),
+                                            ctypes.byref(cells)))
+        return n.value, ms.value, cells.value
+
     def set_model(self, vp, vs, rho, damp_x, damp_z):
         args = [t.to(self.device, torch.float32).contiguous() for t in (vp, vs, rho, damp_x, damp_z)]
         N.check(self.lib.pyfwi_set_model(self.handle, self.ws, self.ws_bytes, *[_ptr(t) for t in args],
