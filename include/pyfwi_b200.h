@@ -170,6 +170,30 @@ int pyfwi_tile_count(int32_t half_order);
 /* Kernel launches this plan issued since creation (for launch accounting). */
 int pyfwi_launch_count(const pyfwi_plan *plan, int64_t *count);
 
+/* Gradient evaluation that allocates no device memory.  No counterpart in
+ * the reference (PyFWI allocates its buffers through pyopencl per
+ * WavePropagator).  For callers that cannot call cudaMalloc -- e.g. a host
+ * program in another language with no CUDA allocator, or an application
+ * whose memory pool owns the whole device -- this runs pyfwi_set_model,
+ * pyfwi_forward, the L2 residual of every observed component and
+ * pyfwi_gradient on one fixed array that the library holds in device memory
+ * (PYFWI_STATIC_SCRATCH_BYTES on every GPU that loads it, until exit).
+ *   vp .. src_vals, n_src   as pyfwi_set_model and pyfwi_forward
+ *   observed  5 device pointers [nt_ext][ns*nr] of observed traces per raw
+ *             component (vx, vz, taux, tauz, tauxz); NULL leaves a component
+ *             out of the misfit
+ *   grad      [3][nz][nx] as pyfwi_gradient;  misfit: device double, overwritten
+ * Plans whose workspace + traces + residuals exceed the array are rejected
+ * (PYFWI_E_WORKSPACE, message gives the bytes needed).  The first call on a
+ * device looks up the array's device address; make it before any stream
+ * capture.  All calls on a device share the array (each call clears what it
+ * needs); calls that overlap on the GPU race. */
+#define PYFWI_STATIC_SCRATCH_BYTES (64u << 20)
+int pyfwi_gradient_static(pyfwi_plan *plan, const float *vp, const float *vs, const float *rho,
+                          const float *damp_x, const float *damp_z, const float *src_vals, int32_t n_src,
+                          const float *const *observed, int32_t parameterization, float *grad, double *misfit,
+                          void *stream);
+
 const char *pyfwi_last_error(void);
 int pyfwi_abi_version(void);
 

@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libpyfwi_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "pyfwi_b200.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "pyfwi_b200.cu"), os.path.join(HERE, "csrc", "static_scratch.cu")]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + \
     [os.path.join(ROOT, "include", "pyfwi_b200.h")]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",

@@ -52,6 +52,10 @@ constexpr int N_TILES = 3;
 
 }  // namespace
 
+// Lets the static-scratch entry point (static_scratch.cu) report through
+// pyfwi_last_error(); hidden from the library's exported symbols.
+__attribute__((visibility("hidden"))) void pyfwi_set_error(const char *msg) { g_err = msg; }
+
 struct pyfwi_plan {
     pyfwi_geometry geom;
     pyfwi_options opt;
@@ -79,6 +83,15 @@ struct pyfwi_plan {
     long long prof_n[3] = {0, 0, 0};
     void *ws_initialised = nullptr;
 };
+
+// Trace dimensions of a plan for the static-scratch entry point; hidden from
+// the library's exported symbols.
+__attribute__((visibility("hidden"))) void pyfwi_plan_trace_dims(const pyfwi_plan *p, int *nt_ext, int *ns, int *nr)
+{
+    *nt_ext = p->geom.nt_ext;
+    *ns = p->geom.ns;
+    *nr = p->geom.nr;
+}
 
 namespace {
 
