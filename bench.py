@@ -19,6 +19,7 @@ reference's loop order on a bounded sample of the same survey, with every
 host thread.
 """
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -296,6 +297,15 @@ def run_ours(args, world, rank, local):
 
     if rank != 0:
         return
+    batched_shots_s = int(W.ns) * args.steps / (ms_max * 1e-3)
+    shape = {"ns": int(W.ns), "nt": int(W.nt), "grid": [int(W.tnz), int(W.tnx)]}
+    layout = {"checkpoint": W.checkpoint, "segment": W.segment, "shot_batch": W.shot_batch}
+    plain = None
+    if world == 1 and args.plain_shots > 0:
+        del step, W, d_obs, g, rms
+        gc.collect()
+        torch.cuda.empty_cache()
+        plain = plain_form(args, dev, batched_shots_s)
     hbm, peak_src = peaks()
     # dominant kernel: the one with the most device time
     kinds = {0: ("fwd_step", BYTES_FWD), 1: ("adj_step", None), 2: ("rev_step", BYTES_FWD)}
@@ -325,15 +335,55 @@ def run_ours(args, world, rank, local):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "shots_per_gpu": int(W.ns), "nt": int(W.nt),
-                       "grid": [int(W.tnz), int(W.tnx)], "checkpoint": W.checkpoint, "segment": W.segment,
-                       "shot_batch": W.shot_batch, "parallelism": "dp%d" % world,
+            "config": {"workload": WORKLOAD, "shots_per_gpu": shape["ns"], "nt": shape["nt"],
+                       "grid": shape["grid"], **layout, "parallelism": "dp%d" % world,
                        "l2": "inputs larger than L2 (no flush)"},
-            "roofline": roof, "cpu_baseline": cpu,
+            "roofline": roof, "cpu_baseline": cpu, "plain": plain,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "clocks": clocks,
             "misfit": float(rms.item())}
     print(json.dumps(line), flush=True)
+
+
+def plain_form(args, dev, batched_shots_s):
+    """The plain form on the same survey: one shot per launch sequence
+    (shot_batch 1) with every forward step stored in FP32 (segment = nt), on
+    the first `--plain-shots` shots.  One untimed evaluation, one timed."""
+    import torch
+    from helpers import product
+    from pyfwi_b200 import fwi_tools
+    case = survey(args.plain_shots, args.nt)
+    extra = {"cuda_device": str(dev), "segment": 0, "shot_batch": 1}
+    if args.tile is not None:
+        extra["tile"] = args.tile
+    W = product(case, **extra)
+    m_est = {k: torch.from_numpy(v).to(dev) for k, v in case["model_est"].items()}
+    m_obs = {k: torch.from_numpy(v).to(dev) for k, v in case["model_obs"].items()}
+    d_obs = {k: v.clone() for k, v in W.forward_modeling(m_obs).items()}
+
+    def step():
+        d_est = W.forward_modeling(m_est)
+        rms, res = fwi_tools.CostFunction("l2")(d_est, d_obs)
+        return W.gradient(res, parameterization="dv"), rms
+
+    step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    shots_s = int(W.ns) / (ms * 1e-3)
+    cells = 2.0 * int(W.tnz) * int(W.tnx) * int(W.nt) * int(W.ns)
+    out = {"shots": int(W.ns), "shot_batch": int(W.shot_batch), "segment": int(W.segment),
+           "snapshots": "fp32, every step", "ms": ms, "shots_per_s": shots_s,
+           "value": cells / (ms * 1e-3) / 1e9, "unit": UNIT, "batched_shots_per_s": batched_shots_s,
+           "batched_over_plain": batched_shots_s / shots_s}
+    del W, d_obs
+    gc.collect()
+    torch.cuda.empty_cache()
+    return out
 
 
 def main():
@@ -348,6 +398,8 @@ def main():
     ap.add_argument("--nt", type=int, default=None, help="shorter record (profiling cases)")
     ap.add_argument("--segment", type=int, default=0, help="steps per recompute segment (default: auto)")
     ap.add_argument("--tile", type=int, default=None, help="kernel tile variant")
+    ap.add_argument("--plain-shots", type=int, default=2,
+                    help="shots of the plain one-shot-per-launch form timed beside the batched one (0: skip)")
     args = ap.parse_args()
     if args.impl == "reference":
         # rank 0 alone times the host CPU; other ranks have nothing to do

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PYFWI_ABI_VERSION 1
+#define PYFWI_ABI_VERSION 3
 
 enum pyfwi_status {
     PYFWI_OK = 0,
@@ -92,6 +92,17 @@ typedef struct pyfwi_geometry {
 } pyfwi_geometry;
 
 /* Run options. */
+/* Which gradient pyfwi_gradient computes.
+ * REFERENCE: PyFWI's adjoint-state gradient (Adj_update_tau, Adj_update_v,
+ *   Grad: elastic.cl:372-526; wave_propagation.py:751-938), masked and
+ *   normalised by gradient_reading.
+ * EXACT: no counterpart in the reference: the exact derivative of
+ *   J = 1/2 sum (trace - observed)^2 of the discrete forward step of this
+ *   library (transposed step, the absorbing profiles held fixed), on the whole
+ *   model grid with no mask; the residual planes are dJ/dtrace per raw trace.
+ *   Needs PYFWI_CKPT_EXACT with FP32 snapshots. */
+enum pyfwi_adjoint { PYFWI_ADJOINT_REFERENCE = 0, PYFWI_ADJOINT_EXACT = 1 };
+
 typedef struct pyfwi_options {
     int32_t checkpoint;     /* enum pyfwi_checkpoint */
     int32_t segment;        /* exact mode: steps per recompute segment; 0 = all steps */
@@ -100,8 +111,13 @@ typedef struct pyfwi_options {
     int32_t energy;         /* 1: also accumulate the energy terms (energy_balancing) */
     int32_t nchp;           /* reverse mode: number of checkpoint steps */
     const int32_t *chp;     /* host; reverse mode: the checkpoint steps (copied) */
-    int32_t tile;           /* kernel tile variant, 0 = default (see pyfwi_tile_count) */
+    int32_t tile;           /* kernel variant (see pyfwi_tile_count): 0..2 tile kernels with
+                               16 / 8 / 32 rows per tile, 3..5 streaming kernels with
+                               128 / 64 / 256 columns per CTA */
     int32_t graph;          /* 1: replay time loops as CUDA graphs */
+    int32_t chunk;          /* streaming kernels: grid rows per CTA, 0 = from the grid size */
+    int32_t adj_tile;       /* adjoint+imaging step variant + 1 (same numbering as tile); 0 = tile */
+    int32_t adjoint;        /* enum pyfwi_adjoint */
 } pyfwi_options;
 
 typedef struct pyfwi_plan pyfwi_plan;
@@ -155,6 +171,15 @@ int pyfwi_l2_residual(const float *est, const float *obs, float *res, int64_t n,
 /* Trace section (acquisition.py:313-333): out = (a + b) / 2 elementwise. */
 int pyfwi_mean2(const float *a, const float *b, float *out, int64_t n, void *stream);
 
+/* Gradient smoothing (the gaussian_filter(g, g_smooth) calls of
+ * wave_propagation.py:923-936): n stacked (nz, nx) device arrays are
+ * correlated along z, then along x, with the 2*radius+1 host weights
+ * (normalised Gaussian), edges extended by half-sample reflection; sums in
+ * double.  tmp: device scratch of n*nz*nx floats, aliasing neither in nor
+ * out (in == out is allowed).  radius <= 127. */
+int pyfwi_smooth(const float *in, float *out, float *tmp, int32_t n, int32_t nz, int32_t nx, const double *weights,
+                 int32_t radius, void *stream);
+
 /* Per-kernel timing.  While enabled, every step kernel the plan launches is
  * bracketed by CUDA events on the caller's stream.  pyfwi_profile_read
  * synchronises on those events and returns, for one kernel kind (0 forward
@@ -169,6 +194,14 @@ int pyfwi_tile_count(int32_t half_order);
 
 /* Kernel launches this plan issued since creation (for launch accounting). */
 int pyfwi_launch_count(const pyfwi_plan *plan, int64_t *count);
+
+/* Read and clear the workspace's device error word after the work queued on
+ * `stream` (synchronises that stream).  *code: 0 none, 1 a streaming kernel
+ * gave up waiting (one second) for a row copy and left its rows unwritten,
+ * 2 a streaming kernel found its shared memory misaligned for copies.
+ * Returns PYFWI_E_TIMEOUT when *code != 0.  The reference has no device-side
+ * waits and no counterpart. */
+int pyfwi_device_error(pyfwi_plan *plan, void *workspace, size_t bytes, int32_t *code, void *stream);
 
 /* Gradient evaluation that allocates no device memory.  No counterpart in
  * the reference (PyFWI allocates its buffers through pyopencl per

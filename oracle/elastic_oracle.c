@@ -560,6 +560,177 @@ int orc_gradient_shot(const orc_cfg *g, const REAL *lam, const REAL *mu, const R
     return 0;
 }
 
+/* ---- exact discrete adjoint (no counterpart in the reference) -----------
+ * The transpose of one forward step of this file (record, source add,
+ * velocity update + damping, stress update + damping, each on the update
+ * domain), so that the gradient it accumulates is the exact derivative of
+ * J = 1/2 sum (traces - observed)^2 with respect to lam, mu and the
+ * buoyancy b on the padded grid, the damping profiles held fixed.  The
+ * transposed differences use (D+)^T = -D- and (D-)^T = -D+ on fields that
+ * are zero outside the update domain; cells outside the grid read as zero
+ * (no flat-index wrap, which only ever reaches constant zero cells in the
+ * forward step). */
+static inline double at0(const REAL *f, const orc_cfg *g, long i, long j)
+{
+    return (i < 0 || i >= g->Nz || j < 0 || j >= g->Nx) ? 0.0 : (double)f[i * g->Nx + j];
+}
+
+static double sfwd(const REAL *f, const orc_cfg *g, long i, long j, int di, int dj, double h)
+{
+    const double c[4] = {g->c1, g->c2, g->c3, g->c4};
+    double s = 0.0;
+    for (int q = 0; q < 4; ++q)
+        s += c[q] * (at0(f, g, i + (q + 1) * di, j + (q + 1) * dj) - at0(f, g, i - q * di, j - q * dj));
+    return s / h;
+}
+
+static double sbwd(const REAL *f, const orc_cfg *g, long i, long j, int di, int dj, double h)
+{
+    const double c[4] = {g->c1, g->c2, g->c3, g->c4};
+    double s = 0.0;
+    for (int q = 0; q < 4; ++q)
+        s += c[q] * (at0(f, g, i + q * di, j + q * dj) - at0(f, g, i - (q + 1) * di, j - (q + 1) * dj));
+    return s / h;
+}
+
+static inline int in_dom(const orc_cfg *g, long i, long j)
+{
+    return i >= g->sdo && i <= (long)g->Nz - g->sdo && j >= g->sdo && j <= (long)g->Nx - g->sdo;
+}
+
+/* Transpose of orc_record for one trace row: add the residual of every trace
+ * slot to the adjoint of the field it recorded (the crosswell vz trace holds
+ * vx, elastic_crosswell.cl:27). */
+static inline void radj5(const orc_cfg *g, orc_state *A, const REAL *const *res, long ir, long cell, int vz_from_vx)
+{
+    REAL *f[5] = {A->vx, vz_from_vx ? A->vx : A->vz, A->taux, A->tauz, A->tauxz};
+    if (ir < 0 || ir >= g->Nr || cell < 0 || cell >= (long)g->Nz * g->Nx) return;
+    for (int k = 0; k < 5; ++k)
+        if (res[k]) f[k][cell] += res[k][ir];
+}
+
+static void record_adjoint(const orc_cfg *g, orc_state *A, const REAL *const *res)
+{
+    const long Nx = g->Nx, Nz = g->Nz;
+    if (g->acq_type == 1 || g->acq_type == 2) {
+        long i = g->rec_surface_const;
+        long off = (g->acq_type == 2) ? g->n_extera_rec : 0;
+        if (i >= 0 && i < Nz)
+            for (long j = 0; j < Nx; j += g->dxr) {
+                long ir = j / g->dxr;
+                if (ir < g->n_main_rec) radj5(g, A, res, off + ir, i * Nx + (j + g->rec_surface_var), 0);
+            }
+    }
+    if (g->acq_type == 0) {
+        long j = g->rec_top_right_const;
+        if (j >= 0 && j < Nx)
+            for (long i = 0; i < Nz; i += g->dxr) radj5(g, A, res, i / g->dxr, (i + g->rec_top_right_var) * Nx + j, 1);
+    }
+    if (g->acq_type == 2) {
+        long j = g->rec_top_left_const;
+        if (j >= 0 && j < Nx)
+            for (long i = 0; i < Nz; i += g->dxr) {
+                long ir = i / g->dxr;
+                if (ir < g->n_extera_rec) radj5(g, A, res, ir, (i + g->rec_top_left_var) * Nx + j, 0);
+            }
+        j = g->rec_top_right_const;
+        long start = g->n_extera_rec + g->n_main_rec;
+        if (j >= 0 && j < Nx)
+            for (long i = 0; i < Nz; i += g->dxr)
+                radj5(g, A, res, start + i / g->dxr, (i + g->rec_top_right_var) * Nx + j, 0);
+    }
+}
+
+/* One shot.  W[t] (t = 0 .. nt-1) is the state after step t, S_{t+1}; S_0 is
+ * zero.  res[5]: this shot's dJ/dtrace planes [nt_ext][Nr] (NULL = zero).
+ * Accumulates dJ/dlam, dJ/dmu, dJ/db on the padded grid into Glam, Gmu, Gb. */
+int orc_exact_gradient_shot(const orc_cfg *g, const REAL *lam, const REAL *mu, const REAL *rho_b, const REAL *dxpml,
+                            const REAL *dzpml, int32_t srcx, int32_t srcz, const float *src_vals, int32_t n_src_vals,
+                            const REAL *const *res, const REAL *W, REAL *Glam, REAL *Gmu, REAL *Gb)
+{
+    const long Nz = g->Nz, Nx = g->Nx, n = Nz * Nx, n5 = 5 * n;
+    const double dt = g->dt;
+    REAL *buf = (REAL *)calloc((size_t)(5 + 5 + 5) * n, sizeof(REAL));
+    if (!buf) return -1;
+    REAL *L = buf;            /* adjoint state, [5][n] */
+    REAL *P = buf + 5 * n;    /* P1, P2, P3, Q1, Q2 */
+    REAL *S0 = buf + 10 * n;  /* S_t with the source added */
+    orc_state A = {L, L + n, L + 2 * n, L + 3 * n, L + 4 * n};
+    REAL *P1 = P, *P2 = P + n, *P3 = P + 2 * n, *Q1 = P + 3 * n, *Q2 = P + 4 * n;
+    for (long t = g->nt - 1; t >= 0; --t) {
+        const REAL *S1 = W + t * n5;
+        if (t > 0)
+            memcpy(S0, W + (t - 1) * n5, (size_t)n5 * sizeof(REAL));
+        else
+            memset(S0, 0, (size_t)n5 * sizeof(REAL));
+        if (t % g->dt_scale == 0 && srcz >= 0 && srcz < Nz && srcx >= 0 && srcx < Nx) {
+            long k = t / g->dt_scale, c = (long)srcz * Nx + srcx;
+            if (k < n_src_vals)
+                for (int f = 0; f < 4; ++f) S0[f * n + c] += src_vals[4 * k + f];
+        }
+        const REAL *vx2 = S1, *vz2 = S1 + n, *txx0 = S0 + 2 * n, *tzz0 = S0 + 3 * n, *txz0 = S0 + 4 * n;
+        /* stress update, transposed: P fields and the lam / mu gradient */
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < Nz; ++i)
+            for (long j = 0; j < Nx; ++j) {
+                long c = i * Nx + j;
+                P1[c] = P2[c] = P3[c] = 0;
+                if (!in_dom(g, i, j)) continue;
+                double damp = 1.0 - dt * ((double)dxpml[c] + (double)dzpml[c]);
+                double axx = damp * A.taux[c], azz = damp * A.tauz[c], axz = damp * A.tauxz[c];
+                double l = lam[c], m = mu[c];
+                P1[c] = (REAL)(dt * ((l + 2 * m) * axx + l * azz));
+                P2[c] = (REAL)(dt * m * axz);
+                P3[c] = (REAL)(dt * (l * axx + (l + 2 * m) * azz));
+                double dxp_vx = sfwd(vx2, g, i, j, 0, 1, g->dx), dzm_vz = sbwd(vz2, g, i, j, 1, 0, g->dz);
+                double dxm_vz = sbwd(vz2, g, i, j, 0, 1, g->dx), dzp_vx = sfwd(vx2, g, i, j, 1, 0, g->dz);
+                Glam[c] += (REAL)(dt * (axx + azz) * (dxp_vx + dzm_vz));
+                Gmu[c] += (REAL)(dt * (2 * axx * dxp_vx + 2 * azz * dzm_vz + axz * (dxm_vz + dzp_vx)));
+                A.taux[c] = (REAL)axx;
+                A.tauz[c] = (REAL)azz;
+                A.tauxz[c] = (REAL)axz;
+            }
+        /* velocity update, transposed: Q fields and the buoyancy gradient */
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < Nz; ++i)
+            for (long j = 0; j < Nx; ++j) {
+                long c = i * Nx + j;
+                double mvx = A.vx[c] - sbwd(P1, g, i, j, 0, 1, g->dx) - sbwd(P2, g, i, j, 1, 0, g->dz);
+                double mvz = A.vz[c] - sfwd(P3, g, i, j, 1, 0, g->dz) - sfwd(P2, g, i, j, 0, 1, g->dx);
+                Q1[c] = Q2[c] = 0;
+                if (in_dom(g, i, j)) {
+                    double damp = 1.0 - dt * ((double)dxpml[c] + (double)dzpml[c]);
+                    double bx = damp * mvx, bz = damp * mvz, b = rho_b[c];
+                    Q1[c] = (REAL)(dt * b * bx);
+                    Q2[c] = (REAL)(dt * b * bz);
+                    Gb[c] += (REAL)(dt * (bx * (sbwd(txx0, g, i, j, 0, 1, g->dx) + sbwd(txz0, g, i, j, 1, 0, g->dz)) +
+                                          bz * (sfwd(tzz0, g, i, j, 1, 0, g->dz) + sfwd(txz0, g, i, j, 0, 1, g->dx))));
+                    mvx = bx;
+                    mvz = bz;
+                }
+                S0[c] = (REAL)mvx; /* S0's vx / vz planes are free scratch now */
+                S0[n + c] = (REAL)mvz;
+            }
+        memcpy(A.vx, S0, (size_t)n * sizeof(REAL));
+        memcpy(A.vz, S0 + n, (size_t)n * sizeof(REAL));
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < Nz; ++i)
+            for (long j = 0; j < Nx; ++j) {
+                long c = i * Nx + j;
+                A.taux[c] = (REAL)(A.taux[c] - sfwd(Q1, g, i, j, 0, 1, g->dx));
+                A.tauz[c] = (REAL)(A.tauz[c] - sbwd(Q2, g, i, j, 1, 0, g->dz));
+                A.tauxz[c] = (REAL)(A.tauxz[c] - sfwd(Q1, g, i, j, 1, 0, g->dz) - sbwd(Q2, g, i, j, 0, 1, g->dx));
+            }
+        if (t % g->dt_scale == 0 && t / g->dt_scale < g->nt_ext) {
+            const REAL *r[5];
+            for (int c = 0; c < 5; ++c) r[c] = res[c] ? res[c] + (t / g->dt_scale) * (long)g->Nr : NULL;
+            record_adjoint(g, &A, r);
+        }
+    }
+    free(buf);
+    return 0;
+}
+
 /* Single-kernel entry points on caller-guarded arrays, for unit checks of one
  * step against the product's kernels. */
 void orc_step_forward(const orc_cfg *g, REAL *vx, REAL *vz, REAL *taux, REAL *tauz, REAL *tauxz, const REAL *lam,

@@ -73,6 +73,8 @@ def lib(precision="fp32"):
                                         P, P, P, P, P, P]
         L.orc_step_forward.restype = None
         L.orc_step_forward.argtypes = [ctypes.POINTER(OrcCfg)] + [P] * 10 + [ctypes.c_int]
+        L.orc_exact_gradient_shot.argtypes = [ctypes.POINTER(OrcCfg), P, P, P, P, P, _i32, _i32, P, _i32,
+                                              ctypes.POINTER(P), P, P, P, P]
         _LIBS[precision] = L
     return _LIBS[precision]
 
@@ -140,10 +142,11 @@ def pml_profiles(tnz, tnx, dh, n_pml, pml_r, pml_dir):
     return dx_pml, dz_pml
 
 
-def expand(param, tnz, tnx, n_pml):
-    """fwi_tools.py:776-811: edge-replicated padding."""
-    nu = np.zeros((tnz, tnx)).astype(np.float32, order="C")
-    nu[n_pml:tnz - n_pml, n_pml:tnx - n_pml] = param.astype(np.float32, order="C")
+def expand(param, tnz, tnx, n_pml, dtype=np.float32):
+    """fwi_tools.py:776-811: edge-replicated padding (float32 as the
+    reference; the FP64 oracle keeps double)."""
+    nu = np.zeros((tnz, tnx)).astype(dtype, order="C")
+    nu[n_pml:tnz - n_pml, n_pml:tnx - n_pml] = param.astype(dtype, order="C")
     nu[:n_pml, :] = nu[n_pml, :]
     nu[tnz - n_pml:, :] = nu[tnz - n_pml - 1, :]
     nu[:, tnx - n_pml:] = nu[:, tnx - n_pml - 1].reshape(-1, 1)
@@ -294,7 +297,7 @@ class OracleWavePropagator:
     def _materials(self, model0):
         model = dict(model0)
         for p in model:
-            model[p] = expand(model[p], self.tnz, self.tnx, self.npml)
+            model[p] = expand(model[p], self.tnz, self.tnx, self.npml, self.real)
         v_max = model["vp"].max()
         vdx = self.dx_pml * v_max
         vdz = self.dz_pml * v_max
@@ -379,6 +382,60 @@ class OracleWavePropagator:
                     "rho": gaussian_filter(grho, self.g_smooth)}
         return {"lam": gaussian_filter(glam, self.g_smooth), "mu": gaussian_filter(gmu, self.g_smooth),
                 "rho": gaussian_filter(grho0, self.g_smooth)}
+
+    # ---- exact discrete adjoint (no counterpart in the reference) -------
+    def raw_traces(self, model0):
+        """Raw receiver traces {field: (nt_ext, nr, ns)} of every shot, in
+        recording order (before any section reshaping or well flip)."""
+        self._materials(model0)
+        out = {f: np.zeros((self.nt_ext, self.nr, self.ns), self.real) for f in FIELDS}
+        for s in range(self.ns):
+            seis, _ = self.forward_shot(s)
+            for k, f in enumerate(FIELDS):
+                out[f][:, :, s] = seis[k]
+        return out
+
+    def exact_gradient(self, model0, dtrace):
+        """dJ/d(lam, mu, b) on the padded grid, summed over shots, for a
+        misfit J of the raw traces with dJ/dtrace = dtrace ({field:
+        (nt_ext, nr, ns)}, missing fields zero), the damping held fixed."""
+        L = lib(self.precision)
+        self._materials(model0)
+        n = (int(self.tnz), int(self.tnx))
+        G = [np.zeros(n, self.real) for _ in range(3)]
+        every = np.arange(self.nt, dtype=np.int32)
+        for s in range(self.ns):
+            seis = np.zeros((5, self.nt_ext, self.nr), self.real)
+            W = np.zeros((self.nt, 5, self.tnz, self.tnx), self.real)
+            L.orc_forward_shot(ctypes.byref(self.cfg), *self._mats(), int(self.srcx[s]), int(self.srcz[s]),
+                               _ptr(self.src_vals), self.n_inj, _ptr(seis), _ptr(W), _ptr(every), self.nt)
+            planes = [np.ascontiguousarray(dtrace[f][:, :, s], self.real) if f in dtrace else None for f in FIELDS]
+            arr = (ctypes.c_void_p * 5)(*[ctypes.c_void_p(p.ctypes.data) if p is not None else None for p in planes])
+            rc = L.orc_exact_gradient_shot(ctypes.byref(self.cfg), *self._mats()[:5], int(self.srcx[s]),
+                                           int(self.srcz[s]), _ptr(self.src_vals), self.n_inj, arr, _ptr(W),
+                                           *[_ptr(g) for g in G])
+            if rc != 0:
+                raise MemoryError("oracle exact gradient: allocation failed")
+        return G
+
+    def model_gradient(self, model0, Glam, Gmu, Gb):
+        """Chain rule from (lam, mu, b) on the padded grid to (vp, vs, rho) on
+        the model grid: lam = rho vp^2 - 2 mu, mu = rho vs^2, b = 1/rho, and
+        the edge-replicated padding folded back onto the edge cells."""
+        R = np.float64
+        vp, vs, rho = (expand(model0[k], self.tnz, self.tnx, self.npml, R) for k in ("vp", "vs", "rho"))
+        Glam, Gmu, Gb = (np.asarray(g, R) for g in (Glam, Gmu, Gb))
+        gp = {"vp": 2 * rho * vp * Glam,
+              "vs": -4 * rho * vs * Glam + 2 * rho * vs * Gmu,
+              "rho": (vp ** 2 - 2 * vs ** 2) * Glam + vs ** 2 * Gmu - Gb / rho ** 2}
+        rows = np.clip(np.arange(self.tnz) - self.npml, 0, self.nz - 1)
+        cols = np.clip(np.arange(self.tnx) - self.npml, 0, self.nx - 1)
+        out = {}
+        for k, g in gp.items():
+            m = np.zeros((int(self.nz), int(self.nx)), R)
+            np.add.at(m, (rows[:, None], cols[None, :]), g)
+            out[k] = m
+        return out
 
     def _gradient_reading(self, Gmu, Glam, Grho, Pmu, Plam, Prho):
         """wave_propagation.py:279-331."""

@@ -14,6 +14,7 @@ _P = ctypes.c_void_p
 PYFWI_OK = 0
 CKPT_EXACT, CKPT_REVERSE = 0, 1
 SNAP_FP32, SNAP_BF16 = 0, 1
+ADJOINT_REFERENCE, ADJOINT_EXACT = 0, 1
 PARAM_LMD, PARAM_DV = 0, 1
 
 
@@ -29,9 +30,13 @@ class Geometry(ctypes.Structure):
                 ("mask_row0", _i32), ("mask_row1", _i32), ("mask_col0", _i32), ("mask_col1", _i32)]
 
 
+ABI_VERSION = 3  # PYFWI_ABI_VERSION of include/pyfwi_b200.h
+
+
 class Options(ctypes.Structure):
     _fields_ = [("checkpoint", _i32), ("segment", _i32), ("snapshot", _i32), ("shot_batch", _i32), ("energy", _i32),
-                ("nchp", _i32), ("chp", ctypes.POINTER(_i32)), ("tile", _i32), ("graph", _i32)]
+                ("nchp", _i32), ("chp", ctypes.POINTER(_i32)), ("tile", _i32), ("graph", _i32), ("chunk", _i32),
+                ("adj_tile", _i32), ("adjoint", _i32)]
 
 
 class NativeError(RuntimeError):
@@ -59,16 +64,22 @@ def lib():
     L.pyfwi_gradient.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(_P), _i32, _P, _P, _P]
     L.pyfwi_l2_residual.argtypes = [_P, _P, _P, ctypes.c_int64, _P, _P]
     L.pyfwi_mean2.argtypes = [_P, _P, _P, ctypes.c_int64, _P]
+    L.pyfwi_smooth.argtypes = [_P, _P, _P, _i32, _i32, _i32, ctypes.POINTER(ctypes.c_double), _i32, _P]
     L.pyfwi_tile_count.argtypes = [_i32]
     L.pyfwi_launch_count.argtypes = [_P, ctypes.POINTER(ctypes.c_int64)]
+    L.pyfwi_device_error.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(_i32), _P]
     L.pyfwi_profile_enable.argtypes = [_P, _i32]
     L.pyfwi_profile_read.argtypes = [_P, _i32, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(ctypes.c_double)]
     L.pyfwi_last_error.restype = ctypes.c_char_p
     L.pyfwi_abi_version.restype = ctypes.c_int
+    if L.pyfwi_abi_version() != ABI_VERSION:
+        raise ImportError("libpyfwi_b200.so has ABI %d, this package needs %d: rebuild with "
+                          "`python -m pyfwi_b200.build`" % (L.pyfwi_abi_version(), ABI_VERSION))
     for name in ("pyfwi_plan_create", "pyfwi_plan_destroy", "pyfwi_workspace_size", "pyfwi_set_model",
                  "pyfwi_forward", "pyfwi_gradient", "pyfwi_l2_residual", "pyfwi_mean2", "pyfwi_tile_count",
-                 "pyfwi_launch_count", "pyfwi_profile_enable", "pyfwi_profile_read"):
+                 "pyfwi_launch_count", "pyfwi_profile_enable", "pyfwi_profile_read", "pyfwi_device_error",
+                 "pyfwi_smooth"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

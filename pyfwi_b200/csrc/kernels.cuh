@@ -15,6 +15,7 @@
 // so stencils never branch on the grid edge.  Arithmetic is FP32 with FMA.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -197,7 +198,24 @@ struct StepArgs {
     int nr;
     int ns;
     Lines lines;
+    int chunk;             // streaming kernels: grid rows per CTA
+    __nv_bfloat16 *snap;   // nullable: BF16 copy of the output state, slot 0
+    long long snap_stride; // elements between the snapshots of consecutive slots
+    const float *tbase;    // streaming kernels: workspace base = row 0 of `tmap`
+    int *err;              // streaming kernels: workspace error word
+    alignas(64) CUtensorMap tmap;  // streaming kernels: the workspace as rows of `pitch` floats
 };
+
+// BF16 copy of the five fields written at cell `co` (round to nearest even).
+__device__ __forceinline__ void write_snap(__nv_bfloat16 *sn, long long P, long long co, float vx, float vz, float txx,
+                                           float tzz, float txz)
+{
+    sn[VX * P + co] = __float2bfloat16_rn(vx);
+    sn[VZ * P + co] = __float2bfloat16_rn(vz);
+    sn[TXX * P + co] = __float2bfloat16_rn(txx);
+    sn[TZZ * P + co] = __float2bfloat16_rn(tzz);
+    sn[TXZ * P + co] = __float2bfloat16_rn(txz);
+}
 
 struct AdjArgs {
     Grid g;
@@ -218,6 +236,10 @@ struct AdjArgs {
     const float *res[5];   // [nt_ext][ns*nr] residual components (nullable)
     int nr, ns;
     Lines lines;
+    int chunk;             // streaming kernels: grid rows per CTA
+    const float *tbase;    // streaming kernels: workspace base = row 0 of `tmap`
+    int *err;              // streaming kernels: workspace error word
+    alignas(64) CUtensorMap tmap;  // streaming kernels: the workspace as rows of `pitch` floats
 };
 
 __device__ __forceinline__ bool in_domain(const Grid &g, int R, int i, int j)
@@ -360,6 +382,7 @@ __global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ Ste
         out[TXX * g.plane + co] = txx;
         out[TZZ * g.plane + co] = tzz;
         out[TXZ * g.plane + co] = txz;
+        if (a.snap) write_snap(a.snap + slot * a.snap_stride, g.plane, co, s_vx[iv], s_vz[iv], txx, tzz, txz);
         if (a.rec_row >= 0) record_cell(a, in, shot, gi, gj);
     }
 }
@@ -681,6 +704,192 @@ __global__ void __launch_bounds__(NTHREADS) adj_step(const __grid_constant__ Adj
 }
 
 // ---------------------------------------------------------------------------
+// exact discrete adjoint (no counterpart in the reference): the transpose of
+// fwd_step, so the accumulated gradient is the exact derivative of
+// J = 1/2 sum (traces - observed)^2 with respect to lam, mu and the buoyancy
+// b, the damping profiles held fixed.  Uses (D+)^T = -D- and (D-)^T = -D+ on
+// fields that vanish outside the update domain.  Per step t, from the adjoint
+// L_{t+1} of S_{t+1}:
+//   a  = (1 - dt d) L_tau                          (stress update, in D)
+//   P1 = dt((lam+2mu) a_xx + lam a_zz), P2 = dt mu a_xz, P3 = dt(lam a_xx + (lam+2mu) a_zz)
+//   m_vx = L_vx - Dx-(P1) - Dz-(P2),  m_vz = L_vz - Dz+(P3) - Dx+(P2)
+//   B  = (1 - dt d) m_v                            (velocity update, in D)
+//   Q1 = dt b B_vx, Q2 = dt b B_vz
+//   L_t: v = B (in D, else m), txx = a - Dx+(Q1), tzz = a - Dz-(Q2), txz = a - Dz+(Q1) - Dx-(Q2)
+//   Glam += dt (a_xx + a_zz)(Dx+ vx + Dz- vz)            [velocities of S_{t+1}]
+//   Gmu  += dt (2 a_xx Dx+ vx + 2 a_zz Dz- vz + a_xz (Dx- vz + Dz+ vx))
+//   Gb   += dt (B_vx (Dx- txx + Dz- txz) + B_vz (Dz+ tzz + Dx+ txz))  [stresses of S_t + source]
+// The trace adjoint (dJ/dtrace into L_t at the receivers) is a separate
+// inject_kernel launch after the step.
+// ---------------------------------------------------------------------------
+struct ExactArgs {
+    Grid g;
+    Coef k;
+    const float *in;        // L_{t+1}, slot 0
+    float *out;             // L_t
+    long long in_stride, out_stride;
+    const float *s1, *s0;   // forward states S_{t+1}, S_t, slot 0 (FP32)
+    long long s1_stride, s0_stride;
+    const float *mat;       // lam, mu, b, rho planes
+    const float *dampx, *dampz;
+    float *gacc;            // [slot][3][plane]: Glam, Gmu, Gb
+    long long gacc_stride;
+    int shot0;
+    const int *srcx, *srcz;
+    float4 src;             // source sample added to S_t at this step
+    int add_src;
+};
+
+// Coefficient of f[j + o] in a backward / forward difference at j.
+template <int R>
+__device__ __forceinline__ float coef_bwd(int o, const float *c)
+{
+    return (o >= 0 && o < R) ? c[o] : ((o < 0 && o >= -R) ? -c[-o - 1] : 0.f);
+}
+
+template <int R>
+__device__ __forceinline__ float coef_fwd(int o, const float *c)
+{
+    return (o >= 1 && o <= R) ? c[o - 1] : ((o <= 0 && o > -R) ? -c[-o] : 0.f);
+}
+
+template <int R, int TZ>
+struct ExactShape {
+    static constexpr int PW = TX + 4 * R, PH = TZ + 4 * R;  // P fields: tile +- 2R
+    static constexpr int QW = TX + 2 * R, QH = TZ + 2 * R;  // Q fields: tile +- R
+    static constexpr int FLOATS = 3 * PW * PH + 2 * QW * QH;
+};
+
+template <int R, int TZ>
+__global__ void __launch_bounds__(NTHREADS) exact_adj_step(const __grid_constant__ ExactArgs a)
+{
+    using S = ExactShape<R, TZ>;
+    constexpr int PW = S::PW, PH = S::PH, QW = S::QW, QH = S::QH;
+    extern __shared__ float4 smem4[];
+    float *p1 = reinterpret_cast<float *>(smem4), *p2 = p1 + PH * PW, *p3 = p2 + PH * PW;
+    float *q1 = p3 + PH * PW, *q2 = q1 + QH * QW;
+
+    const Grid &g = a.g;
+    const long long P = g.plane;
+    const int slot = blockIdx.z, shot = a.shot0 + slot;
+    const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TZ;
+    const float *L1 = a.in + slot * a.in_stride;
+    float *L0 = a.out + slot * a.out_stride;
+    const float *S1 = a.s1 + slot * a.s1_stride, *S0 = a.s0 + slot * a.s0_stride;
+    float *G = a.gacc + slot * a.gacc_stride;
+    const float dt = a.k.dt;
+
+    // stress update, transposed
+    for (int e = threadIdx.x; e < PH * PW; e += NTHREADS) {
+        const int r = e / PW, c = e - r * PW, i = i0 - 2 * R + r, j = j0 - 2 * R + c;
+        float v1 = 0.f, v2 = 0.f, v3 = 0.f;
+        if (in_domain(g, R, i, j)) {
+            const long long co = cell_off(g, i, j);
+            const float damp = 1.f - dt * (__ldg(a.dampx + j + XO) + __ldg(a.dampz + i + ZO));
+            const float axx = damp * __ldg(L1 + TXX * P + co), azz = damp * __ldg(L1 + TZZ * P + co),
+                        axz = damp * __ldg(L1 + TXZ * P + co);
+            const float lam = __ldg(a.mat + co), mu = __ldg(a.mat + P + co), l2m = lam + 2.f * mu;
+            v1 = dt * (l2m * axx + lam * azz);
+            v2 = dt * (mu * axz);
+            v3 = dt * (lam * axx + l2m * azz);
+        }
+        p1[e] = v1;
+        p2[e] = v2;
+        p3[e] = v3;
+    }
+    __syncthreads();
+
+    // velocity update, transposed
+    for (int e = threadIdx.x; e < QH * QW; e += NTHREADS) {
+        const int r = e / QW, c = e - r * QW, i = i0 - R + r, j = j0 - R + c;
+        float v1 = 0.f, v2 = 0.f;
+        if (in_domain(g, R, i, j)) {
+            const long long co = cell_off(g, i, j);
+            const int ip = (r + R) * PW + c + R;
+            const float mvx = __ldg(L1 + VX * P + co) - dbwd<R>(p1, ip, 1, a.k.cx) - dbwd<R>(p2, ip, PW, a.k.cz);
+            const float mvz = __ldg(L1 + VZ * P + co) - dfwd<R>(p3, ip, PW, a.k.cz) - dfwd<R>(p2, ip, 1, a.k.cx);
+            const float damp = 1.f - dt * (__ldg(a.dampx + j + XO) + __ldg(a.dampz + i + ZO));
+            const float b = __ldg(a.mat + 2 * P + co);
+            v1 = dt * (b * (damp * mvx));
+            v2 = dt * (b * (damp * mvz));
+        }
+        q1[e] = v1;
+        q2[e] = v2;
+    }
+    __syncthreads();
+
+    // the tile: L_t and the gradients
+    const int si = a.add_src ? a.srcz[shot] : -(1 << 30), sj = a.srcx[shot];
+    for (int e = threadIdx.x; e < TZ * TX; e += NTHREADS) {
+        const int r = e / TX, c = e - r * TX, i = i0 + r, j = j0 + c;
+        if (i >= g.tnz || j >= g.tnx) continue;
+        const long long co = cell_off(g, i, j);
+        const int ip = (r + 2 * R) * PW + c + 2 * R, iq = (r + R) * QW + c + R;
+        const bool dom = in_domain(g, R, i, j);
+        const float damp = dom ? 1.f - dt * (__ldg(a.dampx + j + XO) + __ldg(a.dampz + i + ZO)) : 1.f;
+        const float mvx = __ldg(L1 + VX * P + co) - dbwd<R>(p1, ip, 1, a.k.cx) - dbwd<R>(p2, ip, PW, a.k.cz);
+        const float mvz = __ldg(L1 + VZ * P + co) - dfwd<R>(p3, ip, PW, a.k.cz) - dfwd<R>(p2, ip, 1, a.k.cx);
+        const float bvx = damp * mvx, bvz = damp * mvz;
+        const float axx = damp * __ldg(L1 + TXX * P + co), azz = damp * __ldg(L1 + TZZ * P + co),
+                    axz = damp * __ldg(L1 + TXZ * P + co);
+        L0[VX * P + co] = bvx;
+        L0[VZ * P + co] = bvz;
+        L0[TXX * P + co] = axx - dfwd<R>(q1, iq, 1, a.k.cx);
+        L0[TZZ * P + co] = azz - dbwd<R>(q2, iq, QW, a.k.cz);
+        L0[TXZ * P + co] = axz - dfwd<R>(q1, iq, QW, a.k.cz) - dbwd<R>(q2, iq, 1, a.k.cx);
+        if (!dom) continue;
+        const long long pz = g.pitch;
+        const float dxp_vx = gfwd<R>(S1 + VX * P, co, 1, a.k.cx), dzm_vz = gbwd<R>(S1 + VZ * P, co, pz, a.k.cz);
+        const float dxm_vz = gbwd<R>(S1 + VZ * P, co, 1, a.k.cx), dzp_vx = gfwd<R>(S1 + VX * P, co, pz, a.k.cz);
+        float dxm_tx = gbwd<R>(S0 + TXX * P, co, 1, a.k.cx), dzm_txz = gbwd<R>(S0 + TXZ * P, co, pz, a.k.cz);
+        float dzp_tz = gfwd<R>(S0 + TZZ * P, co, pz, a.k.cz);
+        const float dxp_txz = gfwd<R>(S0 + TXZ * P, co, 1, a.k.cx);
+        if (si == i) dxm_tx = fmaf(coef_bwd<R>(sj - j, a.k.cx), a.src.z, dxm_tx);  // S_t + source
+        if (sj == j) dzp_tz = fmaf(coef_fwd<R>(si - i, a.k.cz), a.src.w, dzp_tz);
+        G[0 * P + co] += dt * (axx + azz) * (dxp_vx + dzm_vz);
+        G[1 * P + co] += dt * (2.f * axx * dxp_vx + 2.f * azz * dzm_vz + axz * (dxm_vz + dzp_vx));
+        G[2 * P + co] += dt * (bvx * (dxm_tx + dzm_txz) + bvz * (dzp_tz + dxp_txz));
+    }
+}
+
+// Exact gradient on the model grid: the three padded accumulators summed
+// over the cells each model cell was copied to (edge-replicated padding,
+// fwi_tools.py:776-811), then the chain rule lam = rho vp^2 - 2 mu,
+// mu = rho vs^2, b = 1/rho.  param 0: (lam, mu, rho) with rho at fixed
+// lam, mu; 1: (vp, vs, rho).
+__global__ void exact_post_kernel(Grid g, int nz, int nx, int npml, const float *gacc, const float *mat, int param,
+                                  float *out)
+{
+    const long long n = (long long)nz * nx, P = g.plane;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e / nx), j = (int)(e - (long long)i * nx);
+        const int r0 = i == 0 ? 0 : i + npml, r1 = i == nz - 1 ? g.tnz - 1 : i + npml;
+        const int c0 = j == 0 ? 0 : j + npml, c1 = j == nx - 1 ? g.tnx - 1 : j + npml;
+        double sl = 0.0, sm = 0.0, sb = 0.0;
+        for (int r = r0; r <= r1; ++r)
+            for (int c = c0; c <= c1; ++c) {
+                const long long co = cell_off(g, r, c);
+                sl += gacc[co];
+                sm += gacc[P + co];
+                sb += gacc[2 * P + co];
+            }
+        const long long cm = cell_off(g, i + npml, j + npml);
+        const double lam = mat[cm], mu = mat[P + cm], rho = mat[3 * P + cm];
+        const double grho_lm = -sb / (rho * rho);  // d/drho at fixed lam, mu: b = 1/rho
+        if (param == 0) {
+            out[e] = (float)sl;
+            out[n + e] = (float)sm;
+            out[2 * n + e] = (float)grho_lm;
+        } else {
+            const double vp = sqrt((lam + 2.0 * mu) / rho), vs = sqrt(mu / rho);
+            out[e] = (float)(2.0 * rho * vp * sl);
+            out[n + e] = (float)(-4.0 * rho * vs * sl + 2.0 * rho * vs * sm);
+            out[2 * n + e] = (float)((vp * vp - 2.0 * vs * vs) * sl + vs * vs * sm + grho_lm);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // set-up and post-processing kernels
 // ---------------------------------------------------------------------------
 
@@ -844,6 +1053,42 @@ __global__ void mean2_kernel(const float *a, const float *b, float *out, long lo
 {
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
         out[k] = __fdiv_rn(__fadd_rn(a[k], b[k]), 2.f);
+}
+
+// Gaussian smoothing of the gradient (gaussian_filter, wave_propagation.py:
+// 923-936): a 1-D correlation with normalised Gaussian weights along one axis
+// of `n` stacked (nz, nx) arrays, edges extended by half-sample reflection
+// (d c b a | a b c d | d c b a), sums in double, result rounded to float.
+constexpr int SMOOTH_MAX_RADIUS = 127;
+struct SmoothWeights {
+    double w[2 * SMOOTH_MAX_RADIUS + 1];
+};
+
+__device__ __forceinline__ int reflect_index(int i, int n)
+{
+    const int p = 2 * n;
+    int m = i % p;
+    if (m < 0) m += p;
+    return m < n ? m : p - 1 - m;
+}
+
+__global__ void smooth_kernel(const float *in, float *out, int n, int nz, int nx, int axis, int radius,
+                              const __grid_constant__ SmoothWeights W)
+{
+    const long long total = (long long)n * nz * nx;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long plane = e / ((long long)nz * nx);
+        const int rem = (int)(e - plane * nz * nx), i = rem / nx, j = rem - i * nx;
+        const float *src = in + plane * nz * nx;
+        double acc = 0.0;
+        for (int k = -radius; k <= radius; ++k) {
+            const float v = axis == 0 ? src[(long long)reflect_index(i + k, nz) * nx + j]
+                                      : src[(long long)i * nx + reflect_index(j + k, nx)];
+            acc += W.w[k + radius] * (double)v;
+        }
+        out[e] = (float)acc;
+    }
 }
 
 }  // namespace pyfwi

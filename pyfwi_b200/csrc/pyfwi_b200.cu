@@ -7,7 +7,9 @@
 // all enqueued on the caller's stream (optionally replayed as a CUDA graph).
 #include "pyfwi_b200.h"
 #include "kernels.cuh"
+#include "stream_kernels.cuh"
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -46,9 +48,19 @@ int fail(int code, const char *fmt, ...)
 constexpr size_t ALIGN = 256;
 size_t up(size_t x, size_t a = ALIGN) { return (x + a - 1) / a * a; }
 
-// tile variants: rows per tile
-constexpr int TILE_TZ[] = {16, 8, 32};
-constexpr int N_TILES = 3;
+// kernel variants: 0..2 tile kernels with 16 / 8 / 32 rows per tile,
+// 3..5 streaming kernels whose CTAs span 128 / 64 / 256 columns
+constexpr int TILE_TZ[] = {16, 8, 32, 0, 0, 0};
+constexpr int STREAM_W[] = {0, 0, 0, 128, 64, 256};
+constexpr int N_TILES = 6;
+constexpr int FWD_PF = 4, ADJ_PF = 2;  // rows the streaming kernels fetch ahead
+constexpr size_t ERR_OFF = 128;         // byte offset of the device error word in the header
+
+// cuTensorMapEncodeTiled, resolved through the runtime so the library does
+// not link the driver API directly
+typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 }  // namespace
 
@@ -64,7 +76,8 @@ struct pyfwi_plan {
     Grid g;
     Coef k;
     Lines lines;
-    int R, tz, nacc, G, ngroups, seg, M, n_inj;
+    int R, tz, st_w, atz, ast_w, chunk_opt, nacc, G, ngroups, seg, M, n_inj;  // a*: adjoint step variant
+    bool exact_adj = false;  // PYFWI_ADJOINT_EXACT
     long long state;  // floats per state (5 planes)
     // workspace offsets in bytes
     size_t o_hdr, o_src, o_mat, o_dampx, o_dampz, o_work, o_adj, o_gacc, o_store, o_store16, total;
@@ -82,6 +95,19 @@ struct pyfwi_plan {
     double prof_ms[3] = {0, 0, 0}, prof_cells[3] = {0, 0, 0};
     long long prof_n[3] = {0, 0, 0};
     void *ws_initialised = nullptr;
+    // CUDA-graph replay of whole calls (options.graph)
+    struct GraphCache {
+        cudaGraphExec_t exec = nullptr;
+        std::vector<uintptr_t> key;
+        long long launches = 0;
+    } gfwd, ggrad;
+    cudaStream_t cap = nullptr;  // capture stream (the caller's may be the legacy default stream)
+    // tensor map of the workspace for the streaming kernels, per box width
+    struct TMap {
+        void *ws = nullptr;
+        int w = 0;
+        alignas(64) CUtensorMap map;
+    } tmaps[2];
 };
 
 // Trace dimensions of a plan for the static-scratch entry point; hidden from
@@ -182,24 +208,145 @@ struct ProfileScope {
     }
 };
 
-int step_fwd(pyfwi_plan *p, const StepArgs &a, int nslots, cudaStream_t s, bool reverse)
+// Rows per CTA of the streaming kernels: the option, or enough row chunks
+// to give about eight CTAs of 128 threads per SM over the launch.
+int stream_chunk(const pyfwi_plan *p, int nslots, int T)
 {
-    ProfileScope prof(p, s, reverse ? 2 : 0, nslots);
-#define CASE(R_, TZ_) \
-    if (p->R == R_ && p->tz == TZ_) return launch_fwd<R_, TZ_>(p, a, nslots, s, reverse);
-    CASE(2, 16) CASE(2, 8) CASE(2, 32) CASE(4, 16) CASE(4, 8) CASE(4, 32)
-#undef CASE
-    return fail(PYFWI_E_INVALID, "no kernel for half order %d, tile rows %d", p->R, p->tz);
+    if (p->chunk_opt > 0) return std::min(p->chunk_opt, p->g.tnz);
+    const int stripes = (p->g.tnx + (T - 2 * p->R) - 1) / (T - 2 * p->R);
+    const long long target = 148LL * 8 * 128 / T;
+    long long per_chunk = (long long)stripes * nslots;
+    int nchunks = (int)std::max(1LL, (target + per_chunk - 1) / per_chunk);
+    int chunk = (p->g.tnz + nchunks - 1) / nchunks;
+    return std::max(chunk, std::min(p->g.tnz, 8 * p->R));
 }
 
-int step_adj(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
+// The workspace as a 2-D tensor of rows of `pitch` floats with a box of
+// W x 1, for the streaming kernels; encoded once per workspace and width.
+int workspace_map(pyfwi_plan *p, const float *ws, int W, CUtensorMap *out)
 {
-    ProfileScope prof(p, s, 1, nslots);
+    pyfwi_plan::TMap *slot = nullptr;
+    for (auto &m : p->tmaps)
+        if (m.ws == ws && m.w == W) {
+            *out = m.map;
+            return PYFWI_OK;
+        }
+    slot = &p->tmaps[p->tmaps[0].ws ? 1 : 0];
+    if (p->tmaps[0].ws && p->tmaps[1].ws) slot = &p->tmaps[0];
+    static EncodeTiled encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn)
+            return fail(PYFWI_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+        encode = reinterpret_cast<EncodeTiled>(fn);
+    }
+    const size_t row = (size_t)p->g.pitch * sizeof(float);
+    cuuint64_t dims[2] = {(cuuint64_t)p->g.pitch, (cuuint64_t)(p->total / row)};
+    cuuint64_t strides[1] = {(cuuint64_t)row};
+    cuuint32_t box[2] = {(cuuint32_t)W, 1}, estr[2] = {1, 1};
+    CUresult r = encode(&slot->map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(ws), dims, strides, box,
+                        estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(PYFWI_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    slot->ws = const_cast<float *>(ws);
+    slot->w = W;
+    *out = slot->map;
+    return PYFWI_OK;
+}
+
+template <int R, int W>
+int launch_fwd_stream(pyfwi_plan *p, StepArgs a, int nslots, cudaStream_t s, const float *ws)
+{
+    using S = FwdRing<R, W, FWD_PF>;
+    a.chunk = stream_chunk(p, nslots, S::T);
+    a.tbase = ws;
+    a.err = reinterpret_cast<int *>(const_cast<char *>(reinterpret_cast<const char *>(ws)) + ERR_OFF);
+    int rc = workspace_map(p, ws, W, &a.tmap);
+    if (rc) return rc;
+    const int iw = S::T - 2 * R;
+    dim3 grid((p->g.tnx + iw - 1) / iw, (p->g.tnz + a.chunk - 1) / a.chunk, nslots);
+    static bool attr = false;
+    if (!attr) {
+        CK(cudaFuncSetAttribute(fwd_stream<R, W, FWD_PF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::BYTES));
+        attr = true;
+    }
+    fwd_stream<R, W, FWD_PF><<<grid, S::T, S::BYTES, s>>>(a);
+    p->launches++;
+    CKL();
+    return PYFWI_OK;
+}
+
+template <int R, int W, bool E>
+int launch_adj_stream_t(pyfwi_plan *p, AdjArgs a, int nslots, cudaStream_t s, const float *ws)
+{
+    using S = AdjRing<R, W, ADJ_PF, E>;
+    if (a.inj_row >= 0) {  // the streaming adjoint reads the residual from its input state
+        // one CTA per shot: receivers of different lines on one cell then add in line order
+        dim3 ig(1, nslots);
+        inject_kernel<<<ig, 256, 0, s>>>(p->g, const_cast<float *>(a.in), a.in_stride, a.shot0, a.inj_row,
+                                         a.res[0], a.res[1], a.res[2], a.res[3], a.res[4], p->lines, a.ns, a.nr, 0);
+        p->launches++;
+        CKL();
+    }
+    a.chunk = stream_chunk(p, nslots, S::T);
+    a.tbase = ws;
+    a.err = reinterpret_cast<int *>(const_cast<char *>(reinterpret_cast<const char *>(ws)) + ERR_OFF);
+    int rc = workspace_map(p, ws, W, &a.tmap);
+    if (rc) return rc;
+    const int iw = S::T - 2 * R;
+    dim3 grid((p->g.tnx + iw - 1) / iw, (p->g.tnz + a.chunk - 1) / a.chunk, nslots);
+    static bool attr = false;
+    if (!attr) {
+        CK(cudaFuncSetAttribute(adj_stream<R, W, ADJ_PF, E>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)S::BYTES));
+        attr = true;
+    }
+    adj_stream<R, W, ADJ_PF, E><<<grid, S::T, S::BYTES, s>>>(a);
+    p->launches++;
+    CKL();
+    return PYFWI_OK;
+}
+
+template <int R, int W>
+int launch_adj_stream(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s, const float *ws)
+{
+    return p->nacc == 6 ? launch_adj_stream_t<R, W, true>(p, a, nslots, s, ws)
+                        : launch_adj_stream_t<R, W, false>(p, a, nslots, s, ws);
+}
+
+int step_fwd(pyfwi_plan *p, const StepArgs &a, int nslots, cudaStream_t s, bool reverse, const float *ws)
+{
+    ProfileScope prof(p, s, reverse ? 2 : 0, nslots);
+    if (p->st_w && !reverse) {
+#define CASE(R_, W_) \
+    if (p->R == R_ && p->st_w == W_) return launch_fwd_stream<R_, W_>(p, a, nslots, s, ws);
+        CASE(2, 128) CASE(2, 64) CASE(2, 256) CASE(4, 128) CASE(4, 64) CASE(4, 256)
+#undef CASE
+    }
+    const int tz = p->tz ? p->tz : 16;  // reverse steps always use the tile kernel
 #define CASE(R_, TZ_) \
-    if (p->R == R_ && p->tz == TZ_) return launch_adj<R_, TZ_>(p, a, nslots, s);
+    if (p->R == R_ && tz == TZ_) return launch_fwd<R_, TZ_>(p, a, nslots, s, reverse);
     CASE(2, 16) CASE(2, 8) CASE(2, 32) CASE(4, 16) CASE(4, 8) CASE(4, 32)
 #undef CASE
-    return fail(PYFWI_E_INVALID, "no kernel for half order %d, tile rows %d", p->R, p->tz);
+    return fail(PYFWI_E_INVALID, "no kernel for half order %d, tile rows %d", p->R, tz);
+}
+
+int step_adj(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s, const float *ws)
+{
+    ProfileScope prof(p, s, 1, nslots);
+    if (p->ast_w) {
+#define CASE(R_, W_) \
+    if (p->R == R_ && p->ast_w == W_) return launch_adj_stream<R_, W_>(p, a, nslots, s, ws);
+        CASE(2, 128) CASE(2, 64) CASE(2, 256) CASE(4, 128) CASE(4, 64) CASE(4, 256)
+#undef CASE
+    }
+#define CASE(R_, TZ_) \
+    if (p->R == R_ && p->atz == TZ_) return launch_adj<R_, TZ_>(p, a, nslots, s);
+    CASE(2, 16) CASE(2, 8) CASE(2, 32) CASE(4, 16) CASE(4, 8) CASE(4, 32)
+#undef CASE
+    return fail(PYFWI_E_INVALID, "no kernel for half order %d, tile rows %d", p->R, p->atz);
 }
 
 int grid_blocks(long long n)
@@ -214,16 +361,34 @@ struct Buf {
     long long stride;  // floats between slots
 };
 
+bool bf16_snaps(const pyfwi_plan *p)
+{
+    return p->opt.checkpoint == PYFWI_CKPT_EXACT && p->opt.snapshot == PYFWI_SNAP_BF16;
+}
+
+// exact mode, per slot of the store: M restart states S_0, S_seg, ...
+// S_{(M-1)seg}, then (FP32 snapshots) the seg states of the segment being
+// imaged.  With BF16 snapshots the segment states live in the BF16 store and
+// the FP32 chain that produces them runs in the two work states.
+long long store_stride(const pyfwi_plan *p) { return (long long)(p->M + (bf16_snaps(p) ? 0 : p->seg)) * p->state; }
+
 // exact mode: where state S_s of the current group lives during a pass
 Buf exact_state(pyfwi_plan *p, void *ws, int s)
 {
     float *store = at<float>(ws, p->o_store);
     float *work = at<float>(ws, p->o_work);
-    long long sstride = (long long)(p->M + p->seg) * p->state;
+    long long sstride = store_stride(p);
     if (s == 0) return {store, sstride};
     if (p->M > 1 && s % p->seg == 0 && s / p->seg <= p->M - 1) return {store + (long long)(s / p->seg) * p->state, sstride};
-    if (s > (p->M - 1) * p->seg) return {store + (long long)(p->M + s - (p->M - 1) * p->seg - 1) * p->state, sstride};
+    if (s > (p->M - 1) * p->seg && !bf16_snaps(p))
+        return {store + (long long)(p->M + s - (p->M - 1) * p->seg - 1) * p->state, sstride};
     return {work + (long long)(s & 1) * p->state, 2 * p->state};
+}
+
+// BF16 snapshot k (state S_{t_lo+k+1} of the segment being imaged)
+__nv_bfloat16 *snap_at(pyfwi_plan *p, void *ws, int k)
+{
+    return at<__nv_bfloat16>(ws, p->o_store16) + (long long)k * p->state;
 }
 
 StepArgs base_step(pyfwi_plan *p, void *ws)
@@ -271,7 +436,10 @@ int exact_pass(pyfwi_plan *p, void *ws, int s0, int n, float *traces, cudaStream
         a.add_src = inj;
         a.src = src_at(p, k);
         a.rec_row = (inj && traces && k < p->geom.nt_ext) ? k : -1;
-        int rc = step_fwd(p, a, n, st, false);
+        const int last_lo = (p->M - 1) * p->seg;
+        a.snap = bf16_snaps(p) && t >= last_lo ? snap_at(p, ws, t - last_lo) : nullptr;
+        a.snap_stride = (long long)p->seg * p->state;
+        int rc = step_fwd(p, a, n, st, false, at<float>(ws, 0));
         if (rc) return rc;
     }
     return PYFWI_OK;
@@ -320,7 +488,7 @@ int reverse_pass(pyfwi_plan *p, void *ws, int s0, int n, float *traces, cudaStre
         a.add_src = inj;
         a.src = src_at(p, k);
         a.rec_row = (inj && traces && k < p->geom.nt_ext) ? k : -1;
-        int rc = step_fwd(p, a, n, st, false);
+        int rc = step_fwd(p, a, n, st, false, at<float>(ws, 0));
         if (rc) return rc;
         cur = out;
         wcur = wnext;
@@ -348,7 +516,7 @@ AdjArgs base_adj(pyfwi_plan *p, void *ws, const float *const *res)
 }
 
 // backward iteration t of the reference loop (wave_propagation.py:814-848)
-int adjoint_iter(pyfwi_plan *p, AdjArgs &a, int t, int &t_src, int &ping, float *adj, int n, cudaStream_t st)
+int adjoint_iter(pyfwi_plan *p, void *ws, AdjArgs &a, int t, int &t_src, int &ping, float *adj, int n, cudaStream_t st)
 {
     if (t % p->geom.dt_scale == 0) {
         int row = t_src - 1;
@@ -361,9 +529,306 @@ int adjoint_iter(pyfwi_plan *p, AdjArgs &a, int t, int &t_src, int &ping, float 
     a.in = adj + (long long)ping * p->state;
     a.out = adj + (long long)(1 - ping) * p->state;
     a.in_stride = a.out_stride = 2 * p->state;
-    int rc = step_adj(p, a, n, st);
+    int rc = step_adj(p, a, n, st, at<float>(ws, 0));
     ping = 1 - ping;
     return rc;
+}
+
+template <int R, int TZ>
+int launch_exact(pyfwi_plan *p, const ExactArgs &a, int nslots, cudaStream_t s)
+{
+    dim3 grid((p->g.tnx + TX - 1) / TX, (p->g.tnz + TZ - 1) / TZ, nslots);
+    const size_t sm = ExactShape<R, TZ>::FLOATS * sizeof(float);
+    static bool attr = false;
+    if (!attr) {
+        CK(cudaFuncSetAttribute(exact_adj_step<R, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        attr = true;
+    }
+    exact_adj_step<R, TZ><<<grid, NTHREADS, sm, s>>>(a);
+    p->launches++;
+    CKL();
+    return PYFWI_OK;
+}
+
+// The exact adjoint of one group (exact checkpoints, FP32 snapshots): for
+// t = nt-1 .. 0 the transposed step from L_{t+1} to L_t with S_{t+1} and S_t
+// from the segment store, then the trace adjoint of step t.
+int exact_backward(pyfwi_plan *p, void *ws, const float *const *residual, int s0, int n, cudaStream_t st)
+{
+    const pyfwi_geometry &G = p->geom;
+    float *adj = at<float>(ws, p->o_adj);
+    float *store = at<float>(ws, p->o_store);
+    const long long sstride = store_stride(p);
+    StepArgs f = base_step(p, ws);
+    f.shot0 = s0;
+    ExactArgs e;
+    memset(&e, 0, sizeof e);
+    e.g = p->g;
+    e.k = p->k;
+    e.mat = at<float>(ws, p->o_mat);
+    e.dampx = at<float>(ws, p->o_dampx);
+    e.dampz = at<float>(ws, p->o_dampz);
+    e.gacc = at<float>(ws, p->o_gacc);
+    e.gacc_stride = (long long)p->nacc * p->g.plane;
+    e.shot0 = s0;
+    e.srcx = at<int>(ws, p->o_src);
+    e.srcz = at<int>(ws, p->o_src) + G.ns;
+    e.in_stride = e.out_stride = 2 * p->state;
+    e.s1_stride = e.s0_stride = sstride;
+    int ping = 0, rc;
+    for (int m = p->M - 1; m >= 0; --m) {
+        const int t_lo = m * p->seg, t_hi = std::min((m + 1) * p->seg, G.nt);
+        if (m < p->M - 1) {  // recompute segment m from its restart state
+            for (int t = t_lo; t < t_hi; ++t) {
+                Buf out = {store + (long long)(p->M + t - t_lo) * p->state, sstride};
+                Buf in = t > t_lo ? Buf{store + (long long)(p->M + t - t_lo - 1) * p->state, sstride}
+                                  : exact_state(p, ws, t);
+                f.in = in.base;
+                f.in_stride = in.stride;
+                f.out = out.base;
+                f.out_stride = out.stride;
+                f.add_src = t % G.dt_scale == 0;
+                f.src = src_at(p, t / G.dt_scale);
+                f.rec_row = -1;
+                rc = step_fwd(p, f, n, st, false, at<float>(ws, 0));
+                if (rc) return rc;
+            }
+        }
+        for (int t = t_hi - 1; t >= t_lo; --t) {
+            Buf s_t = t > t_lo ? Buf{store + (long long)(p->M + t - t_lo - 1) * p->state, sstride}
+                               : exact_state(p, ws, t);
+            e.s1 = store + (long long)(p->M + t - t_lo) * p->state;
+            e.s0 = s_t.base;
+            e.s0_stride = s_t.stride;
+            e.add_src = t % G.dt_scale == 0;
+            e.src = src_at(p, t / G.dt_scale);
+            e.in = adj + (long long)ping * p->state;
+            e.out = adj + (long long)(1 - ping) * p->state;
+            {
+                ProfileScope prof(p, st, 1, n);
+#define CASE(R_) \
+    if (p->R == R_) rc = launch_exact<R_, 16>(p, e, n, st);
+                rc = PYFWI_E_INVALID;
+                CASE(2) CASE(4)
+#undef CASE
+                if (rc) return rc;
+            }
+            const int row = t / G.dt_scale;
+            if (t % G.dt_scale == 0 && row < G.nt_ext) {
+                inject_kernel<<<dim3(1, n), 256, 0, st>>>(p->g, e.out, 2 * p->state, s0, row, residual[0], residual[1],
+                                                          residual[2], residual[3], residual[4], p->lines, G.ns, G.nr,
+                                                          1);
+                p->launches++;
+                CKL();
+            }
+            ping = 1 - ping;
+        }
+    }
+    return PYFWI_OK;
+}
+
+// Everything pyfwi_gradient enqueues (host state is updated by the caller).
+int gradient_enqueue(pyfwi_plan *p, void *ws, const float *const *residual, int32_t param, float *grad, float *raw,
+                     cudaStream_t st)
+{
+    int rc;
+    const pyfwi_geometry &G = p->geom;
+    float *gacc = at<float>(ws, p->o_gacc);
+    float *adj = at<float>(ws, p->o_adj);
+    CK(cudaMemsetAsync(gacc, 0, (size_t)p->nacc * p->g.plane * p->G * sizeof(float), st));
+    AdjArgs a = base_adj(p, ws, residual);
+
+    for (int grp = 0; grp < p->ngroups; ++grp) {
+        int s0 = grp * p->G, n = std::min(p->G, G.ns - s0);
+        a.shot0 = s0;
+        for (int q = 0; q < n; ++q) CK(cudaMemsetAsync(adj + 2 * q * p->state, 0, p->state * sizeof(float), st));
+        int ping = 0, t_src = G.nt_ext;
+        if (p->exact_adj) {
+            if (p->ngroups > 1 || !p->fwd_valid) {
+                rc = exact_pass(p, ws, s0, n, nullptr, st);
+                if (rc) return rc;
+            }
+            const float *zero[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+            rc = exact_backward(p, ws, residual ? residual : zero, s0, n, st);
+            if (rc) return rc;
+        } else if (p->opt.checkpoint == PYFWI_CKPT_EXACT) {
+            if (p->ngroups > 1 || !p->fwd_valid) {
+                rc = exact_pass(p, ws, s0, n, nullptr, st);
+                if (rc) return rc;
+            }
+            StepArgs f = base_step(p, ws);
+            f.shot0 = s0;
+            for (int m = p->M - 1; m >= 0; --m) {
+                int t_lo = m * p->seg, t_hi = std::min((m + 1) * p->seg, G.nt);
+                if (m < p->M - 1) {  // recompute segment m from its restart state
+                    for (int t = t_lo; t < t_hi; ++t) {
+                        Buf in = exact_state(p, ws, t), out;
+                        if (bf16_snaps(p)) {
+                            out = work_state(p, ws, (t + 1) & 1);
+                            if (t > t_lo) in = work_state(p, ws, t & 1);
+                            f.snap = snap_at(p, ws, t - t_lo);
+                            f.snap_stride = (long long)p->seg * p->state;
+                        } else {
+                            out = {at<float>(ws, p->o_store) + (long long)(p->M + t - t_lo) * p->state,
+                                   store_stride(p)};
+                            if (t > t_lo)
+                                in = {at<float>(ws, p->o_store) + (long long)(p->M + t - t_lo - 1) * p->state,
+                                      out.stride};
+                        }
+                        f.in = in.base;
+                        f.in_stride = in.stride;
+                        f.out = out.base;
+                        f.out_stride = out.stride;
+                        bool inj = t % G.dt_scale == 0;
+                        f.add_src = inj;
+                        f.src = src_at(p, t / G.dt_scale);
+                        f.rec_row = -1;
+                        rc = step_fwd(p, f, n, st, false, at<float>(ws, 0));
+                        if (rc) return rc;
+                    }
+                }
+                for (int t = t_hi - 1; t >= std::max(t_lo, 1); --t) {
+                    // forward state after step t: S_{t+1}
+                    if (bf16_snaps(p)) {
+                        a.fwd = nullptr;
+                        a.fwd16 = snap_at(p, ws, t - t_lo);
+                        a.fwd_stride = (long long)p->seg * p->state;
+                    } else {
+                        a.fwd = at<float>(ws, p->o_store) + (long long)(p->M + t - t_lo) * p->state;
+                        a.fwd_stride = store_stride(p);
+                    }
+                    rc = adjoint_iter(p, ws, a, t, t_src, ping, adj, n, st);
+                    if (rc) return rc;
+                }
+            }
+        } else {
+            // reference chpr < 100 scheme (wave_propagation.py:761-812)
+            int nchp = (int)p->chp.size(), chpc = nchp - 1, wlast = 1;
+            Buf cur = {nullptr, 0};
+            StepArgs f = base_step(p, ws);
+            f.shot0 = s0;
+            for (int t = G.nt - 1; t > 0; --t) {
+                int kk = chpc >= 0 ? chpc : chpc + nchp;
+                if (t == p->chp[kk]) {
+                    cur = chp_state(p, ws, s0, kk);
+                    chpc -= 1;
+                } else {
+                    if (!cur.base) return fail(PYFWI_E_STATE, "reverse schedule has no starting checkpoint");
+                    int w = 1 - wlast;
+                    Buf out = work_state(p, ws, w);
+                    f.in = cur.base;
+                    f.in_stride = cur.stride;
+                    f.out = out.base;
+                    f.out_stride = out.stride;
+                    rc = step_fwd(p, f, n, st, true, at<float>(ws, 0));
+                    if (rc) return rc;
+                    cur = out;
+                    wlast = w;
+                }
+                a.fwd = cur.base;
+                a.fwd_stride = cur.stride;
+                rc = adjoint_iter(p, ws, a, t, t_src, ping, adj, n, st);
+                if (rc) return rc;
+            }
+        }
+    }
+
+    const long long nplane = (long long)p->nacc * p->g.plane;
+    if (p->G > 1) {
+        reduce_slots_kernel<<<grid_blocks(nplane), 256, 0, st>>>(gacc, nplane, p->G, nplane);
+        p->launches++;
+        CKL();
+    }
+    if (raw) {
+        if (p->nacc < 6)
+            CK(cudaMemsetAsync(raw, 0, 6 * (size_t)p->g.tnz * p->g.tnx * sizeof(float), st));
+        raw_out_kernel<<<grid_blocks((long long)p->nacc * p->g.tnz * p->g.tnx), 256, 0, st>>>(p->g, gacc, p->nacc, raw);
+        p->launches++;
+        CKL();
+    }
+    if (p->exact_adj) {
+        const long long nm = (long long)G.nz * G.nx;
+        exact_post_kernel<<<grid_blocks(nm), 256, 0, st>>>(p->g, G.nz, G.nx, G.npml, gacc, at<float>(ws, p->o_mat),
+                                                           param == PYFWI_PARAM_DV ? 1 : 0, grad);
+        p->launches++;
+        CKL();
+        return PYFWI_OK;
+    }
+    PostArgs pa;
+    pa.g = p->g;
+    pa.nz = G.nz;
+    pa.nx = G.nx;
+    pa.npml = G.npml;
+    pa.r0 = G.mask_row0;
+    pa.r1 = G.mask_row1;
+    pa.c0 = G.mask_col0;
+    pa.c1 = G.mask_col1;
+    pa.energy = p->nacc == 6;
+    pa.param = param;
+    pa.gacc = gacc;
+    pa.mat = at<float>(ws, p->o_mat);
+    pa.fmax_bits = at<int>(ws, p->o_hdr) + 4;
+    pa.out = grad;
+    CK(cudaMemsetAsync(pa.fmax_bits, 0, 3 * sizeof(int), st));
+    long long nm = (long long)G.nz * G.nx;
+    factor_max_kernel<<<grid_blocks(nm), 256, 0, st>>>(pa);
+    p->launches++;
+    CKL();
+    post_kernel<<<grid_blocks(nm), 256, 0, st>>>(pa);
+    p->launches++;
+    CKL();
+    return PYFWI_OK;
+}
+
+int forward_enqueue(pyfwi_plan *p, void *ws, float *traces, cudaStream_t st)
+{
+    if (traces)
+        CK(cudaMemsetAsync(traces, 0, 5 * (size_t)p->geom.nt_ext * p->geom.ns * p->geom.nr * sizeof(float), st));
+    for (int grp = 0; grp < p->ngroups; ++grp) {
+        int s0 = grp * p->G, n = std::min(p->G, p->geom.ns - s0);
+        int rc = p->opt.checkpoint == PYFWI_CKPT_EXACT ? exact_pass(p, ws, s0, n, traces, st)
+                                                         : reverse_pass(p, ws, s0, n, traces, st);
+        if (rc) return rc;
+    }
+    return PYFWI_OK;
+}
+
+// Replay `enqueue` as a CUDA graph: captured once per distinct key (the
+// pointers and values the launches bake in) on the plan's own stream, then
+// launched on the caller's stream.
+template <typename F>
+int run_graph(pyfwi_plan *p, pyfwi_plan::GraphCache &c, const std::vector<uintptr_t> &key, cudaStream_t st,
+              F enqueue)
+{
+    if (!c.exec || c.key != key) {
+        if (c.exec) {
+            cudaGraphExecDestroy(c.exec);
+            c.exec = nullptr;
+        }
+        if (!p->cap) CK(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
+        const long long l0 = p->launches;
+        CK(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue(p->cap);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(p->cap, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (e != cudaSuccess) return fail(PYFWI_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&c.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            c.exec = nullptr;
+            return fail(PYFWI_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        }
+        c.key = key;
+        c.launches = p->launches - l0;
+        p->launches = l0;
+    }
+    CK(cudaGraphLaunch(c.exec, st));
+    p->launches += c.launches;
+    return PYFWI_OK;
 }
 
 }  // namespace
@@ -408,8 +873,18 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
                 return fail(PYFWI_E_INVALID, "checkpoint steps must be increasing and inside [0, nt)");
         if (opt->chp[opt->nchp - 1] != G.nt - 1) return fail(PYFWI_E_INVALID, "last checkpoint must be step nt-1");
     }
-    if (opt->snapshot == PYFWI_SNAP_BF16) return fail(PYFWI_E_INVALID, "bf16 snapshots are not enabled in this build");
+    if (opt->snapshot != PYFWI_SNAP_FP32 && opt->snapshot != PYFWI_SNAP_BF16)
+        return fail(PYFWI_E_INVALID, "unknown snapshot format");
+    if (opt->snapshot == PYFWI_SNAP_BF16 && opt->checkpoint != PYFWI_CKPT_EXACT)
+        return fail(PYFWI_E_INVALID, "bf16 snapshots need the exact checkpoint mode");
     if (opt->tile < 0 || opt->tile >= N_TILES) return fail(PYFWI_E_INVALID, "tile variant out of range");
+    if (opt->adj_tile < 0 || opt->adj_tile > N_TILES) return fail(PYFWI_E_INVALID, "adj_tile out of range");
+    if (opt->adjoint != PYFWI_ADJOINT_REFERENCE && opt->adjoint != PYFWI_ADJOINT_EXACT)
+        return fail(PYFWI_E_INVALID, "unknown adjoint kind");
+    if (opt->adjoint == PYFWI_ADJOINT_EXACT &&
+        (opt->checkpoint != PYFWI_CKPT_EXACT || opt->snapshot != PYFWI_SNAP_FP32 || opt->energy))
+        return fail(PYFWI_E_INVALID, "the exact adjoint needs exact checkpoints, FP32 snapshots and no energy terms");
+    if (opt->chunk < 0) return fail(PYFWI_E_INVALID, "chunk must be >= 0");
 
     pyfwi_plan *p = new pyfwi_plan();
     p->geom = G;
@@ -420,7 +895,17 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
     p->opt.chp = nullptr;
     p->R = G.half_order;
     p->tz = TILE_TZ[opt->tile];
+    p->st_w = STREAM_W[opt->tile];
+    const int av = opt->adj_tile ? opt->adj_tile - 1 : opt->tile;
+    p->atz = TILE_TZ[av];
+    p->ast_w = STREAM_W[av];
+    if (opt->snapshot == PYFWI_SNAP_BF16 && p->ast_w) {  // BF16 snapshots are read by the tile adjoint kernel
+        p->ast_w = 0;
+        p->atz = TILE_TZ[0];
+    }
+    p->chunk_opt = opt->chunk;
     p->nacc = opt->energy ? 6 : 3;
+    p->exact_adj = opt->adjoint == PYFWI_ADJOINT_EXACT;
     p->g.tnz = tnz;
     p->g.tnx = tnx;
     p->g.pitch = (int)up((size_t)tnx + 2 * XO, 32);
@@ -451,29 +936,41 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
     p->n_inj = (G.nt + G.dt_scale - 1) / G.dt_scale;
 
     const size_t pf = (size_t)p->g.plane * sizeof(float), sb = (size_t)p->state * sizeof(float);
+    // regions holding planes start on a row of the workspace (a multiple of
+    // the row bytes and of ALIGN), so every plane is a run of whole rows of
+    // the workspace tensor the streaming kernels copy from
+    const size_t rowb = (size_t)p->g.pitch * sizeof(float), ra = rowb % ALIGN ? rowb * 2 : rowb;
+    auto upr = [ra](size_t x) { return (x + ra - 1) / ra * ra; };
     size_t o = 0;
     p->o_hdr = o;
     o += ALIGN;
     p->o_src = o;
     o += up(2 * (size_t)G.ns * sizeof(int));
+    o = upr(o);
     p->o_mat = o;
     o += up(4 * pf);
     p->o_dampx = o;
     o += up((size_t)p->g.pitch * sizeof(float));
     p->o_dampz = o;
     o += up((size_t)p->g.rows * sizeof(float));
+    o = upr(o);
     p->o_work = o;
     o += up(2 * sb * p->G);
+    o = upr(o);
     p->o_adj = o;
     o += up(2 * sb * p->G);
+    o = upr(o);
     p->o_gacc = o;
     o += up((size_t)p->nacc * pf * p->G);
+    o = upr(o);
     p->o_store = o;
     if (opt->checkpoint == PYFWI_CKPT_EXACT)
-        o += up((size_t)(p->M + p->seg) * sb * p->G);
+        o += up((size_t)store_stride(p) * sizeof(float) * p->G);
     else
         o += up(p->chp.size() * sb * G.ns);
+    o = upr(o);
     p->o_store16 = o;
+    if (bf16_snaps(p)) o += up((size_t)p->seg * p->state * sizeof(__nv_bfloat16) * p->G);
     p->total = o;
     *out = p;
     return PYFWI_OK;
@@ -481,11 +978,15 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
 
 int pyfwi_plan_destroy(pyfwi_plan *plan)
 {
-    if (plan)
+    if (plan) {
         for (auto &e : plan->events) {
             cudaEventDestroy(e.a);
             cudaEventDestroy(e.b);
         }
+        if (plan->gfwd.exec) cudaGraphExecDestroy(plan->gfwd.exec);
+        if (plan->ggrad.exec) cudaGraphExecDestroy(plan->ggrad.exec);
+        if (plan->cap) cudaStreamDestroy(plan->cap);
+    }
     delete plan;
     return PYFWI_OK;
 }
@@ -535,6 +1036,22 @@ int pyfwi_launch_count(const pyfwi_plan *p, int64_t *count)
     return PYFWI_OK;
 }
 
+int pyfwi_device_error(pyfwi_plan *p, void *ws, size_t bytes, int32_t *code, void *stream)
+{
+    if (!p || !code) return fail(PYFWI_E_INVALID, "NULL argument");
+    int rc = check_ws(p, ws, bytes);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int32_t v = 0;
+    int *word = at<int>(ws, ERR_OFF);
+    CK(cudaMemcpyAsync(&v, word, sizeof v, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemsetAsync(word, 0, sizeof v, st));
+    CK(cudaStreamSynchronize(st));
+    *code = v;
+    if (v) return fail(PYFWI_E_TIMEOUT, "device error word %d: a streaming kernel stopped early", v);
+    return PYFWI_OK;
+}
+
 int pyfwi_set_model(pyfwi_plan *p, void *ws, size_t bytes, const float *vp, const float *vs, const float *rho,
                     const float *damp_x, const float *damp_z, void *stream)
 {
@@ -578,14 +1095,16 @@ int pyfwi_forward(pyfwi_plan *p, void *ws, size_t bytes, const float *src_vals, 
     if (!p->model_set) return fail(PYFWI_E_STATE, "pyfwi_set_model must come first");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     p->src_vals.assign(src_vals, src_vals + 4 * (size_t)n_src);
-    if (traces)
-        CK(cudaMemsetAsync(traces, 0, 5 * (size_t)p->geom.nt_ext * p->geom.ns * p->geom.nr * sizeof(float), st));
-    for (int grp = 0; grp < p->ngroups; ++grp) {
-        int s0 = grp * p->G, n = std::min(p->G, p->geom.ns - s0);
-        rc = p->opt.checkpoint == PYFWI_CKPT_EXACT ? exact_pass(p, ws, s0, n, traces, st)
-                                                     : reverse_pass(p, ws, s0, n, traces, st);
-        if (rc) return rc;
+    std::vector<uintptr_t> key = {reinterpret_cast<uintptr_t>(ws), reinterpret_cast<uintptr_t>(traces)};
+    for (float v : p->src_vals) {
+        uint32_t b;
+        memcpy(&b, &v, 4);
+        key.push_back(b);
     }
+    rc = p->opt.graph && !p->profiling
+             ? run_graph(p, p->gfwd, key, st, [&](cudaStream_t s) { return forward_enqueue(p, ws, traces, s); })
+             : forward_enqueue(p, ws, traces, st);
+    if (rc) return rc;
     p->fwd_valid = true;
     return PYFWI_OK;
 }
@@ -598,123 +1117,21 @@ int pyfwi_gradient(pyfwi_plan *p, void *ws, size_t bytes, const float *const *re
     if (rc) return rc;
     if (!p->fwd_valid) return fail(PYFWI_E_STATE, "pyfwi_gradient needs a pyfwi_forward of the current model first");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const pyfwi_geometry &G = p->geom;
-    float *gacc = at<float>(ws, p->o_gacc);
-    float *adj = at<float>(ws, p->o_adj);
-    CK(cudaMemsetAsync(gacc, 0, (size_t)p->nacc * p->g.plane * p->G * sizeof(float), st));
-    AdjArgs a = base_adj(p, ws, residual);
-
-    for (int grp = 0; grp < p->ngroups; ++grp) {
-        int s0 = grp * p->G, n = std::min(p->G, G.ns - s0);
-        a.shot0 = s0;
-        for (int q = 0; q < n; ++q) CK(cudaMemsetAsync(adj + 2 * q * p->state, 0, p->state * sizeof(float), st));
-        int ping = 0, t_src = G.nt_ext;
-        if (p->opt.checkpoint == PYFWI_CKPT_EXACT) {
-            if (p->ngroups > 1 || !p->fwd_valid) {
-                rc = exact_pass(p, ws, s0, n, nullptr, st);
-                if (rc) return rc;
-            }
-            StepArgs f = base_step(p, ws);
-            f.shot0 = s0;
-            for (int m = p->M - 1; m >= 0; --m) {
-                int t_lo = m * p->seg, t_hi = std::min((m + 1) * p->seg, G.nt);
-                if (m < p->M - 1) {  // recompute segment m from its restart state
-                    for (int t = t_lo; t < t_hi; ++t) {
-                        Buf in = exact_state(p, ws, t);
-                        Buf out = {at<float>(ws, p->o_store) + (long long)(p->M + t - t_lo) * p->state,
-                                   (long long)(p->M + p->seg) * p->state};
-                        if (t > t_lo)
-                            in = {at<float>(ws, p->o_store) + (long long)(p->M + t - t_lo - 1) * p->state, out.stride};
-                        f.in = in.base;
-                        f.in_stride = in.stride;
-                        f.out = out.base;
-                        f.out_stride = out.stride;
-                        bool inj = t % G.dt_scale == 0;
-                        f.add_src = inj;
-                        f.src = src_at(p, t / G.dt_scale);
-                        f.rec_row = -1;
-                        rc = step_fwd(p, f, n, st, false);
-                        if (rc) return rc;
-                    }
-                }
-                for (int t = t_hi - 1; t >= std::max(t_lo, 1); --t) {
-                    // forward state after step t: S_{t+1}
-                    a.fwd = at<float>(ws, p->o_store) + (long long)(p->M + t - t_lo) * p->state;
-                    a.fwd_stride = (long long)(p->M + p->seg) * p->state;
-                    rc = adjoint_iter(p, a, t, t_src, ping, adj, n, st);
-                    if (rc) return rc;
-                }
-            }
-        } else {
-            // reference chpr < 100 scheme (wave_propagation.py:761-812)
-            int nchp = (int)p->chp.size(), chpc = nchp - 1, wlast = 1;
-            Buf cur = {nullptr, 0};
-            StepArgs f = base_step(p, ws);
-            f.shot0 = s0;
-            for (int t = G.nt - 1; t > 0; --t) {
-                int kk = chpc >= 0 ? chpc : chpc + nchp;
-                if (t == p->chp[kk]) {
-                    cur = chp_state(p, ws, s0, kk);
-                    chpc -= 1;
-                } else {
-                    if (!cur.base) return fail(PYFWI_E_STATE, "reverse schedule has no starting checkpoint");
-                    int w = 1 - wlast;
-                    Buf out = work_state(p, ws, w);
-                    f.in = cur.base;
-                    f.in_stride = cur.stride;
-                    f.out = out.base;
-                    f.out_stride = out.stride;
-                    rc = step_fwd(p, f, n, st, true);
-                    if (rc) return rc;
-                    cur = out;
-                    wlast = w;
-                }
-                a.fwd = cur.base;
-                a.fwd_stride = cur.stride;
-                rc = adjoint_iter(p, a, t, t_src, ping, adj, n, st);
-                if (rc) return rc;
-            }
-        }
+    std::vector<uintptr_t> key = {reinterpret_cast<uintptr_t>(ws), reinterpret_cast<uintptr_t>(grad),
+                                  reinterpret_cast<uintptr_t>(raw), (uintptr_t)param, (uintptr_t)p->fwd_valid};
+    for (int c = 0; c < 5; ++c) key.push_back(reinterpret_cast<uintptr_t>(residual ? residual[c] : nullptr));
+    for (float v : p->src_vals) {
+        uint32_t b;
+        memcpy(&b, &v, 4);
+        key.push_back(b);
     }
+    rc = p->opt.graph && !p->profiling
+             ? run_graph(p, p->ggrad, key, st,
+                         [&](cudaStream_t s) { return gradient_enqueue(p, ws, residual, param, grad, raw, s); })
+             : gradient_enqueue(p, ws, residual, param, grad, raw, st);
+    if (rc) return rc;
     if (p->opt.checkpoint == PYFWI_CKPT_EXACT && p->M > 1) p->fwd_valid = false;  // last segment overwritten
     if (p->opt.checkpoint == PYFWI_CKPT_EXACT && p->ngroups > 1) p->fwd_valid = true;  // passes were redone anyway
-
-    const long long nplane = (long long)p->nacc * p->g.plane;
-    if (p->G > 1) {
-        reduce_slots_kernel<<<grid_blocks(nplane), 256, 0, st>>>(gacc, nplane, p->G, nplane);
-        p->launches++;
-        CKL();
-    }
-    if (raw) {
-        if (p->nacc < 6)
-            CK(cudaMemsetAsync(raw, 0, 6 * (size_t)p->g.tnz * p->g.tnx * sizeof(float), st));
-        raw_out_kernel<<<grid_blocks((long long)p->nacc * p->g.tnz * p->g.tnx), 256, 0, st>>>(p->g, gacc, p->nacc, raw);
-        p->launches++;
-        CKL();
-    }
-    PostArgs pa;
-    pa.g = p->g;
-    pa.nz = G.nz;
-    pa.nx = G.nx;
-    pa.npml = G.npml;
-    pa.r0 = G.mask_row0;
-    pa.r1 = G.mask_row1;
-    pa.c0 = G.mask_col0;
-    pa.c1 = G.mask_col1;
-    pa.energy = p->nacc == 6;
-    pa.param = param;
-    pa.gacc = gacc;
-    pa.mat = at<float>(ws, p->o_mat);
-    pa.fmax_bits = at<int>(ws, p->o_hdr) + 4;
-    pa.out = grad;
-    CK(cudaMemsetAsync(pa.fmax_bits, 0, 3 * sizeof(int), st));
-    long long nm = (long long)G.nz * G.nx;
-    factor_max_kernel<<<grid_blocks(nm), 256, 0, st>>>(pa);
-    p->launches++;
-    CKL();
-    post_kernel<<<grid_blocks(nm), 256, 0, st>>>(pa);
-    p->launches++;
-    CKL();
     return PYFWI_OK;
 }
 
@@ -723,6 +1140,26 @@ int pyfwi_l2_residual(const float *est, const float *obs, float *res, int64_t n,
     if (!est || !obs || !res || !misfit || n < 0) return fail(PYFWI_E_INVALID, "bad argument");
     if (n == 0) return PYFWI_OK;
     l2_kernel<<<grid_blocks(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(est, obs, res, n, misfit);
+    CKL();
+    return PYFWI_OK;
+}
+
+int pyfwi_smooth(const float *in, float *out, float *tmp, int32_t n, int32_t nz, int32_t nx, const double *weights,
+                 int32_t radius, void *stream)
+{
+    if (!in || !out || !tmp || !weights || n < 0 || nz < 1 || nx < 1) return fail(PYFWI_E_INVALID, "bad argument");
+    if (radius < 0 || radius > SMOOTH_MAX_RADIUS)
+        return fail(PYFWI_E_INVALID, "smoothing radius %d outside [0, %d]", radius, SMOOTH_MAX_RADIUS);
+    if (n == 0) return PYFWI_OK;
+    if (tmp == in || tmp == out) return fail(PYFWI_E_INVALID, "tmp must not alias in or out");
+    SmoothWeights w;
+    memset(&w, 0, sizeof w);
+    for (int k = 0; k <= 2 * radius; ++k) w.w[k] = weights[k];
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const long long total = (long long)n * nz * nx;
+    smooth_kernel<<<grid_blocks(total), 256, 0, st>>>(in, tmp, n, nz, nx, 0, radius, w);
+    CKL();
+    smooth_kernel<<<grid_blocks(total), 256, 0, st>>>(tmp, out, n, nz, nx, 1, radius, w);
     CKL();
     return PYFWI_OK;
 }

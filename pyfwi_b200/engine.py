@@ -85,6 +85,13 @@ class Plan:
         N.check(self.lib.pyfwi_launch_count(self.handle, ctypes.byref(c)))
         return c.value
 
+    def check_device(self):
+        """Synchronise the device stream and raise NativeError if a streaming
+        kernel gave up waiting for a row copy since the last check."""
+        code = ctypes.c_int32()
+        N.check(self.lib.pyfwi_device_error(self.handle, self.ws, self.ws_bytes, ctypes.byref(code),
+                                            _stream(self.device)))
+
     def profile(self, enable=True):
         """Bracket every step kernel with CUDA events (see profile_read)."""
         N.check(self.lib.pyfwi_profile_enable(self.handle, 1 if enable else 0))
@@ -115,17 +122,38 @@ class Plan:
 
     def gradient(self, residual, param, grad=None, raw=None):
         """residual: list of 5 device tensors [nt_ext, ns*nr] or None.
-        Returns grad [3, nz, nx] (float32, device)."""
+        Returns grad [3, nz, nx] (float32, device).
+
+        With graph replay on, the residual is copied into buffers the plan
+        keeps, so every call presents the same pointers to the captured
+        graph."""
         res = []
-        for r in residual:
-            res.append(None if r is None else r.to(self.device, torch.float32).contiguous())
+        for q, r in enumerate(residual):
+            if r is None:
+                res.append(None)
+                continue
+            r = r.to(self.device, torch.float32)
+            if self.opts.graph:
+                buf = self._res_bufs.get(q) if hasattr(self, "_res_bufs") else None
+                if buf is None or buf.shape != r.shape:
+                    if not hasattr(self, "_res_bufs"):
+                        self._res_bufs = {}
+                    buf = self._res_bufs[q] = torch.empty_like(r, memory_format=torch.contiguous_format)
+                buf.copy_(r)
+                r = buf
+            res.append(r.contiguous())
         arr = (ctypes.c_void_p * 5)(*[(r.data_ptr() if r is not None else None) for r in res])
         if grad is None:
-            grad = torch.empty((3, self.nz, self.nx), dtype=torch.float32, device=self.device)
+            if self.opts.graph:
+                if getattr(self, "_grad_buf", None) is None:
+                    self._grad_buf = torch.empty((3, self.nz, self.nx), dtype=torch.float32, device=self.device)
+                grad = self._grad_buf
+            else:
+                grad = torch.empty((3, self.nz, self.nx), dtype=torch.float32, device=self.device)
         N.check(self.lib.pyfwi_gradient(self.handle, self.ws, self.ws_bytes, arr, int(param), _ptr(grad), _ptr(raw),
                                         _stream(self.device)))
         self._res_keep = res
-        return grad
+        return grad.clone() if self.opts.graph else grad
 
 
 def mean2(a, b):
@@ -134,6 +162,32 @@ def mean2(a, b):
     b = b.contiguous()
     out = torch.empty_like(a)
     N.check(N.lib().pyfwi_mean2(_ptr(a), _ptr(b), _ptr(out), a.numel(), _stream(a.device)))
+    return out
+
+
+def gaussian_weights(sigma, truncate=4.0):
+    """Normalised Gaussian weights of scipy.ndimage.gaussian_filter1d
+    (radius int(truncate * sigma + 0.5)), in double."""
+    sigma = float(sigma)
+    radius = int(truncate * sigma + 0.5)
+    x = np.arange(-radius, radius + 1, dtype=np.float64)
+    w = np.exp(-0.5 / (sigma * sigma) * x ** 2)
+    return w / w.sum(), radius
+
+
+def smooth(planes, sigma):
+    """Gaussian smoothing of stacked (n, nz, nx) float32 device arrays with
+    standard deviation `sigma` cells, returned as a new tensor; sigma <= 1e-15
+    returns a copy (gaussian_filter leaves the array unchanged then)."""
+    x = planes.contiguous()
+    if float(sigma) <= 1e-15:
+        return x.clone()
+    w, radius = gaussian_weights(sigma)
+    n, nz, nx = x.shape
+    out = torch.empty_like(x)
+    tmp = torch.empty_like(x)
+    N.check(N.lib().pyfwi_smooth(_ptr(x), _ptr(out), _ptr(tmp), int(n), int(nz), int(nx),
+                                 w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), int(radius), _stream(x.device)))
     return out
 
 

@@ -12,8 +12,20 @@ torch tensors (outputs stay on the device).
 
 Extra ``inpa`` keys (all optional): ``checkpoint`` ('exact' or 'reverse';
 default: 'exact' when chpr == 100, else the reference's reverse-time scheme),
-``segment`` (steps per recompute segment), ``shot_batch``, ``tile`` (kernel
-variant), ``device``-independent ``cuda_device`` (torch device string).
+``segment`` (steps per recompute segment), ``shot_batch``, ``tile`` (step
+kernel variant, 0..5, or 'auto' to time them all on this survey first and
+take the fastest forward and adjoint variant), ``adj_tile`` (adjoint step
+variant when it differs from ``tile``), ``chunk`` (rows per CTA of the
+streaming variants), ``graph`` (replay whole calls as CUDA graphs),
+``snapshot`` ('fp32', or 'bf16': the forward states the imaging reads are
+stored in BF16 while the forward recurrence stays FP32; halves their memory
+and their reads at the cost of rounding the imaged fields to 8 bits),
+``adjoint`` ('reference': PyFWI's gradient, masked and normalised as
+gradient_reading does; 'exact': the exact derivative of
+J = 1/2 sum (section - observed)^2 of this library's discrete forward step on
+the whole model grid, with ``res`` read as dJ/d(section), the absorbing
+profiles held fixed; needs checkpoint 'exact'),
+``cuda_device`` (torch device string).
 """
 import warnings
 
@@ -23,10 +35,11 @@ import torch
 from . import _native as N
 from . import acquisition as acq
 from . import fwi_tools as tools
-from .engine import Plan, mean2
+from .engine import Plan, mean2, smooth
 from .processing import COMPONENTS
 
 FIELDS = COMPONENTS
+DEFAULT_TILE = 0  # step kernel variant when inpa has no 'tile'
 
 
 def _slice_bounds(start, stop, n):
@@ -120,6 +133,18 @@ class WavePreparation:
         if self._plan is None:
             self._build_plan(self.inpa)
         return self._plan
+
+    @property
+    def tile(self):
+        """Forward step kernel variant of the plan (builds it)."""
+        self.plan  # noqa: B018 (builds the plan)
+        return self._tile
+
+    @property
+    def adj_tile(self):
+        """Adjoint step kernel variant of the plan (builds it)."""
+        self.plan  # noqa: B018 (builds the plan)
+        return self._adj_tile
 
     # ---- geometry for the native plan --------------------------------------
     def _lines(self):
@@ -228,7 +253,8 @@ class WavePreparation:
         return vals
 
     def _build_plan(self, inpa):
-        mode = inpa.get("checkpoint", "exact" if self.chpr == 100 else "reverse")
+        exact_default = self.chpr == 100 or inpa.get("adjoint") == "exact"
+        mode = inpa.get("checkpoint", "exact" if exact_default else "reverse")
         if mode not in ("exact", "reverse"):
             raise ValueError("inpa['checkpoint'] must be 'exact' or 'reverse'")
         self.checkpoint = mode
@@ -241,22 +267,42 @@ class WavePreparation:
             o = N.Options()
             o.checkpoint = N.CKPT_EXACT if mode == "exact" else N.CKPT_REVERSE
             o.segment = int(seg)
-            o.snapshot = N.SNAP_FP32
+            o.snapshot = snapshot
             o.shot_batch = int(batch)
             o.energy = 1 if self.energy_balancing else 0
-            o.tile = int(inpa.get("tile", 0))
-            o.graph = 0
+            o.tile, o.adj_tile = variants
+            o.adjoint = N.ADJOINT_EXACT if self.adjoint == "exact" else N.ADJOINT_REFERENCE
+            o.graph = int(bool(inpa.get("graph", False)))
+            o.chunk = int(inpa.get("chunk", 0))
             if chp is not None:
                 o.nchp = int(chp.size)
                 o.chp = chp.ctypes.data_as(N.ctypes.POINTER(N.ctypes.c_int32))
             return o
 
+        self.adjoint = inpa.get("adjoint", "reference")
+        if self.adjoint not in ("reference", "exact"):
+            raise ValueError("inpa['adjoint'] must be 'reference' or 'exact'")
+        if self.adjoint == "exact" and (mode != "exact" or self.energy_balancing):
+            raise ValueError("inpa['adjoint'] = 'exact' needs checkpoint 'exact' and no energy balancing")
+        snap = inpa.get("snapshot", "fp32")
+        if snap not in ("fp32", "bf16") or (snap == "bf16" and mode != "exact"):
+            raise ValueError("inpa['snapshot'] must be 'fp32' or 'bf16' (bf16 with checkpoint 'exact' only)")
+        snapshot = N.SNAP_BF16 if snap == "bf16" else N.SNAP_FP32
+        self.snapshot = snap
+        tile = inpa.get("tile", DEFAULT_TILE)
+        adj_tile = inpa.get("adj_tile", None)
+        variants = (0 if tile == "auto" else int(tile), 0 if adj_tile is None else int(adj_tile) + 1)
         seg = int(inpa.get("segment", 0))
         batch = int(inpa.get("shot_batch", 0))
         if mode == "exact" and ("segment" not in inpa or "shot_batch" not in inpa):
             seg, batch = self._auto_layout(geom, opts, seg, batch)
+        if tile == "auto":
+            from .autotune import tune
+            fwd, adj, _ = tune(geom, srcx, srcz, self.energy_balancing, batch or int(self.ns), self.device)
+            variants = (fwd, adj + 1)
         self._plan = Plan(geom, srcx, srcz, opts(seg, batch), self.device, chp=chp)
         self.segment, self.shot_batch = seg, batch
+        self._tile, self._adj_tile = variants[0], (variants[1] - 1 if variants[1] else variants[0])
 
     def _auto_layout(self, geom, opts, seg, batch):
         """Largest segment (fewest recomputed steps) and shot batch whose
@@ -310,9 +356,17 @@ class WavePropagator(WavePreparation):
         self._traces = self.plan.forward(self._wavelet, self._traces)
         self._model_dev = (vp, vs, rho)
         data = self._section(self._traces)
+        self._check_device(as_numpy)
         if as_numpy:
             data = {k: v.cpu().numpy() for k, v in data.items()}
         return data
+
+    def _check_device(self, synchronous):
+        """Raise if a streaming kernel stopped early.  Reading the error word
+        synchronises, so it is done where the call synchronises anyway (host
+        results) or where a streaming kernel ran."""
+        if synchronous or self.plan.opts.tile >= 3:
+            self.plan.check_device()
 
     def _section(self, traces):
         """acquisition.seismic_section on device traces [5][nt_ext][ns*nr]."""
@@ -350,8 +404,6 @@ class WavePropagator(WavePreparation):
         Returns {'vp','vs','rho'} ('dv') or {'lam','mu','rho'}."""
         if show:
             warnings.warn("show=True: live wavefield plotting is not available; ignored")
-        if self.g_smooth:
-            raise NotImplementedError("gradient smoothing (g_smooth > 0) is not provided")
         as_numpy = not isinstance(res[[*res][0]], torch.Tensor)
         nt, nrs = int(self.nt_ext), int(self.nr) * int(self.ns)
         planes = []
@@ -364,13 +416,35 @@ class WavePropagator(WavePreparation):
                 r = (np.transpose(r, (0, 2, 1)) if isinstance(r, np.ndarray) else r.permute(0, 2, 1))
             r = self._to_device(r).reshape(nt, nrs).contiguous()
             planes.append(r)
+        if self.adjoint == "exact":
+            planes = self._trace_adjoint(planes)
         param = N.PARAM_DV if parameterization == "dv" else N.PARAM_LMD
         g = self.plan.gradient(planes, param)
+        if float(self.g_smooth) > 1e-15:  # gaussian_filter(., g_smooth) per parameter (:923-936)
+            g = smooth(g, self.g_smooth)
         names = ("vp", "vs", "rho") if parameterization == "dv" else ("lam", "mu", "rho")
         out = {n: g[q] for q, n in enumerate(names)}
+        self._check_device(as_numpy)
         if as_numpy:
             out = {k: v.cpu().numpy() for k, v in out.items()}
         return out
+
+    def _trace_adjoint(self, planes):
+        """Exact adjoint: the section's dJ/d(section) per key -> dJ/d(raw
+        trace) per field.  components 0 records (taux + tauz) / 2 under both
+        keys, so each raw stress trace gets half the sum; acquisition 2 lists
+        the left-well traces in reverse, a permutation undone here."""
+        P = list(planes)
+        if self.components == 0 and (P[2] is not None or P[3] is not None):
+            tx = P[2] if P[2] is not None else torch.zeros_like(P[3])
+            tz = P[3] if P[3] is not None else torch.zeros_like(P[2])
+            P[2] = P[3] = mean2(tx, tz)
+        if self.acq_type == 2 and self.n_well_rec:
+            ns, nr, nw = int(self.ns), int(self.nr), int(self.n_well_rec)
+            idx = torch.arange(ns * nr, device=self.device).view(ns, nr)
+            idx[:, :nw] = idx[:, :nw].flip(1)
+            P = [None if p is None else p.index_select(1, idx.reshape(-1)).contiguous() for p in P]
+        return P
 
     def raw_gradient(self, res):
         """The six (tnz, tnx) accumulators (Gmu, Glam, Grho and the energy
@@ -378,4 +452,5 @@ class WavePropagator(WavePreparation):
         planes = [None if k not in res else self._to_device(res[k]).contiguous() for k in FIELDS]
         raw = torch.zeros((6, int(self.tnz), int(self.tnx)), dtype=torch.float32, device=self.device)
         self.plan.gradient(planes, N.PARAM_LMD, raw=raw)
+        self._check_device(True)
         return raw

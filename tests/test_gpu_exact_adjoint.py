@@ -1,0 +1,106 @@
+"""The exact adjoint on the GPU (inpa['adjoint'] = 'exact').
+
+1. Against the FP64 oracle's exact gradient (oracle/elastic_oracle.c,
+   orc_exact_gradient_shot, itself pinned to central finite differences by
+   test_oracle_exact_adjoint.py) on every small case, within the gradient
+   tolerance 1e-4.
+2. Through the torch.autograd.Function (torchfwi.Fwi) on the 200 x 400-cell
+   two-layer survey: <dJ/dm, d> against central finite differences of the
+   misfit with eps = 1e-3 (relative) on 32 seeded random directions, with the
+   reference's gradient's agreement stated beside it."""
+import numpy as np
+import pytest
+from scipy.ndimage import gaussian_filter
+
+import cases
+from conftest import rel_l2
+from helpers import fp64_propagator, product
+
+pytestmark = pytest.mark.gpu
+
+GRAD_TOL = 1e-4
+FIELDS = ["vx", "vz", "taux", "tauz", "tauxz"]
+SECTION = {0: ["taux", "tauz"], 1: ["taux"], 2: ["vx", "vz"], 3: ["taux", "tauz", "tauxz"], 4: FIELDS}
+
+
+def _fp64_exact(case):
+    """FP64 oracle: exact model gradient of J = 1/2 sum (section - observed)^2."""
+    W = fp64_propagator(case)
+    m_obs = {k: v.astype(np.float64) for k, v in case["model_obs"].items()}
+    m_est = {k: v.astype(np.float64) for k, v in case["model_est"].items()}
+    obs, est = W.raw_traces(m_obs), W.raw_traces(m_est)
+    comp = case["components"]
+    if comp == 0:  # both section keys hold (taux + tauz) / 2
+        r = (est["taux"] + est["tauz"] - obs["taux"] - obs["tauz"]) / 2
+        dtr = {"taux": r, "tauz": r}
+    else:
+        dtr = {k: est[k] - obs[k] for k in SECTION[comp]}
+    return W.model_gradient(m_est, *W.exact_gradient(m_est, dtr))
+
+
+@pytest.mark.parametrize("name", [f.__name__ for f in cases.TINY])
+def test_exact_gradient_matches_fp64_oracle(name):
+    case = cases.by_name(name)
+    W = product(case, adjoint="exact")
+    d_obs = W.forward_modeling(case["model_obs"])
+    d_est = W.forward_modeling(case["model_est"])
+    grad = W.gradient({k: d_est[k] - d_obs[k] for k in d_est}, parameterization="dv")
+    ref = _fp64_exact(case)
+    for k in ("vp", "vs", "rho"):
+        assert rel_l2(grad[k], ref[k]) <= GRAD_TOL, (k, rel_l2(grad[k], ref[k]))
+
+
+def _directions(shape, vp, n, eps, seed=2024):
+    """n seeded smooth random directions for (vp, vs, rho), each scaled to a
+    maximum of 1, zero wherever the perturbation could raise max(vp) (the
+    absorbing profiles scale with it)."""
+    rng = np.random.default_rng(seed)
+    keep = vp * (1 + 3 * eps) < vp.max()
+    out = []
+    for _ in range(n):
+        d = {}
+        for k in ("vp", "vs", "rho"):
+            f = gaussian_filter(rng.standard_normal(shape), 10.0)
+            d[k] = (f / np.abs(f).max() * keep).astype(np.float32)
+        out.append(d)
+    return out
+
+
+def test_autograd_gradient_matches_central_differences():
+    import torch
+    from pyfwi_b200.torchfwi import Fwi
+    case = cases.c2()
+    eps, ndir = 1e-3, 32
+    dev = torch.device("cuda", 0)
+    W = product(case, adjoint="exact")
+    m0 = {k: torch.from_numpy(v).to(dev) for k, v in case["model_est"].items()}
+    obs = W.forward_modeling({k: torch.from_numpy(v).to(dev) for k, v in case["model_obs"].items()})
+    obs = (obs["taux"].clone(), obs["tauz"].clone())
+
+    def misfit(m):
+        tx, tz = Fwi.apply(W, m["vp"], m["vs"], m["rho"])
+        return 0.5 * ((tx.double() - obs[0].double()) ** 2).sum() + 0.5 * ((tz.double() - obs[1].double()) ** 2).sum()
+
+    leaves = {k: v.clone().requires_grad_(True) for k, v in m0.items()}
+    misfit(leaves).backward()
+    grad = {k: v.grad.double() for k, v in leaves.items()}
+    # the reference's gradient on the same residual, for comparison only
+    Wr = product(case)
+    d = Wr.forward_modeling(m0)
+    gref = Wr.gradient({k: d[k] - o for k, o in zip(("taux", "tauz"), obs)})
+
+    rel, rel_ref = [], []
+    with torch.no_grad():
+        for d in _directions(case["model_est"]["vp"].shape, case["model_est"]["vp"], ndir, eps):
+            dm = {k: eps * m0[k] * torch.from_numpy(d[k]).to(dev) for k in d}
+            jp = float(misfit({k: m0[k] + dm[k] for k in m0}))
+            jm = float(misfit({k: m0[k] - dm[k] for k in m0}))
+            fd = (jp - jm) / 2
+            pred = sum(float((grad[k] * dm[k].double()).sum()) for k in dm)
+            pred_ref = sum(float((gref[k].double() * dm[k].double()).sum()) for k in dm)
+            rel.append(abs(pred - fd) / abs(fd))
+            rel_ref.append(abs(pred_ref - fd) / abs(fd))
+    rel, rel_ref = np.array(rel), np.array(rel_ref)
+    print("\nFD check, %d directions, eps %.0e: exact adjoint median %.2e max %.2e | reference gradient median %.2e"
+          % (ndir, eps, np.median(rel), rel.max(), np.median(rel_ref)))
+    assert np.median(rel) < 1e-3 and rel.max() < 1e-2, rel

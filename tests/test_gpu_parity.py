@@ -22,11 +22,15 @@ def _golden_section(g, prefix):
     return {k[len(prefix):]: g[k] for k in g if k.startswith(prefix)}
 
 
+VARIANTS = [0, 3, 4, 5]  # tile kernel (64 x 16) and the streaming kernels (128 / 64 / 256 columns)
+
+
+@pytest.mark.parametrize("tile", VARIANTS)
 @pytest.mark.parametrize("name", NAMES)
-def test_forward_and_gradient_match_reference(name):
+def test_forward_and_gradient_match_reference(name, tile):
     g = load_golden(name)
     case = cases.by_name(name)
-    W = product(case)
+    W = product(case, tile=tile)
     d_obs = W.forward_modeling(case["model_obs"])
     for k, v in d_obs.items():
         assert v.dtype == np.float32 and v.shape == g["d_obs_" + k].shape
@@ -81,16 +85,71 @@ def test_exact_checkpoint_segments_are_bit_identical():
 
 
 def test_tile_variants_agree():
+    """Tile kernels of every height give identical bits; streaming kernels
+    (other FMA grouping) agree to float32 rounding."""
     case = cases.tiny_dxr()
     base = None
-    for tile in range(3):
+    for tile in range(6):
         W = product(case, tile=tile)
         d = W.forward_modeling(case["model_est"])
         if base is None:
             base = d
-        else:
-            for k in d:
+        for k in d:
+            if tile < 3:
                 assert np.array_equal(d[k], base[k]), (tile, k)
+            else:
+                assert rel_l2(d[k], base[k]) < 1e-6, (tile, k)
+
+
+@pytest.mark.parametrize("chunk", [3, 8, 1000])
+def test_streaming_row_chunks_agree(chunk):
+    """Splitting the rows among CTAs does not change the result."""
+    case = cases.tiny_s8()
+    g = load_golden("tiny_s8")
+    W = product(case, tile=3, chunk=chunk)
+    d = W.forward_modeling(case["model_est"])
+    for k, v in d.items():
+        assert rel_l2(v, g["d_est_" + k]) < SEIS_TOL, k
+    res = l2_residual_np(_golden_section(g, "d_est_"), _golden_section(g, "d_obs_"))
+    grad = W.gradient(res, parameterization="lmd")
+    for k, v in grad.items():
+        assert rel_l2(v, g["grad_" + k]) < GRAD_TOL, k
+
+
+@pytest.mark.parametrize("fwd,adj", [(0, 3), (3, 0), (4, 5)])
+def test_mixed_forward_and_adjoint_variants(fwd, adj):
+    """A forward variant and a different adjoint variant in one plan."""
+    case = cases.tiny_s8()
+    g = load_golden("tiny_s8")
+    W = product(case, tile=fwd, adj_tile=adj)
+    assert (W.tile, W.adj_tile) == (fwd, adj)
+    d = W.forward_modeling(case["model_est"])
+    for k, v in d.items():
+        assert rel_l2(v, g["d_est_" + k]) < SEIS_TOL, k
+    res = l2_residual_np(_golden_section(g, "d_est_"), _golden_section(g, "d_obs_"))
+    grad = W.gradient(res, parameterization="lmd")
+    for k, v in grad.items():
+        assert rel_l2(v, g["grad_" + k]) < GRAD_TOL, k
+
+
+def test_autotuned_variants():
+    """tile='auto' times every variant on the survey and runs the fastest
+    forward and adjoint kernels; the result still matches the reference."""
+    from pyfwi_b200 import autotune
+    case = cases.tiny_chpr()
+    g = load_golden("tiny_chpr")
+    W = product(case, tile="auto")
+    n = 6
+    assert 0 <= W.tile < n and 0 <= W.adj_tile < n
+    tables = [t for (_, _, t) in autotune._CACHE.values()]
+    assert any(sorted(t) == list(range(n)) and all(a > 0 and b > 0 for a, b in t.values()) for t in tables)
+    d = W.forward_modeling(case["model_est"])
+    for k, v in d.items():
+        assert rel_l2(v, g["d_est_" + k]) < SEIS_TOL, k
+    res = l2_residual_np(_golden_section(g, "d_est_"), _golden_section(g, "d_obs_"))
+    grad = W.gradient(res, parameterization="lmd")
+    for k, v in grad.items():
+        assert rel_l2(v, g["grad_" + k]) < GRAD_TOL, k
 
 
 def test_tensor_inputs_stay_on_device():

@@ -91,3 +91,15 @@ def test_geometry_struct_rounds_constants_like_the_reference_macros():
     g = W._geometry()
     assert g.half_order == 4 and abs(g.c[0] - 1.195955) < 1e-7 and abs(g.c[3] + 0.000697) < 1e-9
     assert np.float32(g.dt) == np.float32(float("%f" % W.dt))
+
+
+def test_gaussian_weights_follow_scipy():
+    """The smoothing weights are scipy's gaussian_filter1d kernel: filtering
+    a unit impulse with them reproduces scipy on the same impulse."""
+    from scipy.ndimage import gaussian_filter1d
+    from pyfwi_b200.engine import gaussian_weights
+    for sigma in (0.5, 1.0, 2.7, 6.0):
+        w, r = gaussian_weights(sigma)
+        x = np.zeros(4 * r + 9)
+        x[2 * r + 4] = 1.0
+        np.testing.assert_allclose(gaussian_filter1d(x, sigma), np.convolve(x, w, mode="same"), rtol=0, atol=1e-15)

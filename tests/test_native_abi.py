@@ -34,7 +34,7 @@ def test_exports_every_declared_symbol(native):
 
 
 def test_abi_version(native):
-    assert native.lib().pyfwi_abi_version() == 1
+    assert native.lib().pyfwi_abi_version() == native.ABI_VERSION == 3
 
 
 def _geom(native, nz=20, nx=24, npml=4, ns=2, nr=10, half=2):
@@ -117,3 +117,22 @@ def test_calls_without_workspace_fail_cleanly(native):
     z = ctypes.c_void_p(1)
     assert L.pyfwi_set_model(h, None, 0, z, z, z, z, z, None) == -2
     L.pyfwi_plan_destroy(h)
+
+
+def _struct_fields(name):
+    text = open(HEADER).read()
+    body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), text, re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    names = []
+    for decl in filter(None, (d.strip() for d in body.split(";"))):
+        declarators = re.match(r"(?:const\s+)?\w+\s*\**\s*(.*)$", decl, re.S).group(1)
+        names += [re.sub(r"[\s*]|\[\w+\]", "", d) for d in declarators.split(",")]
+    return names
+
+
+@pytest.mark.parametrize("cname,pyname", [("pyfwi_options", "Options"), ("pyfwi_geometry", "Geometry"),
+                                          ("pyfwi_rec_line", "RecLine")])
+def test_ctypes_structs_follow_the_header(native, cname, pyname):
+    """The ctypes mirrors list the header's fields in the header's order."""
+    fields = [f[0] for f in getattr(native, pyname)._fields_]
+    assert fields == _struct_fields(cname)

@@ -3,11 +3,13 @@ by running PyFWI's WavePropagator and its kernels, tests/golden/make_golden.py).
 
 The oracle restates the reference arithmetic operation for operation, so the
 fp32 oracle must reproduce the fixtures bit for bit."""
+import os
+
 import numpy as np
 import pytest
 
 import cases
-from conftest import load_golden, rel_l2
+from conftest import GOLDEN, load_golden, rel_l2
 from helpers import oracle_run
 
 TINY = [f.__name__ for f in cases.TINY]
@@ -68,3 +70,14 @@ def test_fp64_oracle_close_to_reference():
         assert rel_l2(v, g["d_est_" + k]) < 1e-5, k
     for k, v in grad.items():
         assert rel_l2(v, g["grad_" + k]) < 1e-3, k
+
+
+def test_fp64_fixtures_reproduce():
+    """The committed FP64 fixtures are what the FP64 oracle computes now."""
+    case = cases.by_name("tiny_dxr")
+    f = np.load(os.path.join(GOLDEN, "tiny_dxr_fp64.npz"))
+    _, d_est, grad, _ = oracle_run(case, precision="fp64")
+    for k, v in d_est.items():
+        assert np.array_equal(np.asarray(v, np.float64), f["d_est_" + k]), k
+    for k, v in grad.items():
+        assert np.array_equal(np.asarray(v, np.float64), f["grad_" + k]), k
