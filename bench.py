@@ -215,7 +215,9 @@ def run_ours(args, world, rank, local):
     if args.segment:
         extra.update(segment=args.segment, shot_batch=args.shots)
     if args.tile is not None:
-        extra["tile"] = args.tile
+        extra["tile"] = args.tile if args.tile == "auto" else int(args.tile)
+    if args.adj_tile is not None:
+        extra["adj_tile"] = args.adj_tile
     W = product(case, **extra)
     ncell = float(int(W.tnz) * int(W.tnx))
     nint = float((int(W.tnz) - 2 * (int(W.npml) + int(W.sdo)) + 1) * (int(W.tnx) - 2 * (int(W.npml) + int(W.sdo)) + 1))
@@ -299,7 +301,8 @@ def run_ours(args, world, rank, local):
         return
     batched_shots_s = int(W.ns) * args.steps / (ms_max * 1e-3)
     shape = {"ns": int(W.ns), "nt": int(W.nt), "grid": [int(W.tnz), int(W.tnx)]}
-    layout = {"checkpoint": W.checkpoint, "segment": W.segment, "shot_batch": W.shot_batch}
+    layout = {"checkpoint": W.checkpoint, "segment": W.segment, "shot_batch": W.shot_batch,
+              "kernels": {"forward": int(W.tile), "adjoint": int(W.adj_tile)}}
     plain = None
     if world == 1 and args.plain_shots > 0:
         del step, W, d_obs, g, rms
@@ -355,7 +358,9 @@ def plain_form(args, dev, batched_shots_s):
     case = survey(args.plain_shots, args.nt)
     extra = {"cuda_device": str(dev), "segment": 0, "shot_batch": 1}
     if args.tile is not None:
-        extra["tile"] = args.tile
+        extra["tile"] = args.tile if args.tile == "auto" else int(args.tile)
+    if args.adj_tile is not None:
+        extra["adj_tile"] = args.adj_tile
     W = product(case, **extra)
     m_est = {k: torch.from_numpy(v).to(dev) for k, v in case["model_est"].items()}
     m_obs = {k: torch.from_numpy(v).to(dev) for k, v in case["model_obs"].items()}
@@ -397,7 +402,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--nt", type=int, default=None, help="shorter record (profiling cases)")
     ap.add_argument("--segment", type=int, default=0, help="steps per recompute segment (default: auto)")
-    ap.add_argument("--tile", type=int, default=None, help="kernel tile variant")
+    ap.add_argument("--tile", default=None, help="step kernel variant 0..5, or 'auto' (autotuner)")
+    ap.add_argument("--adj-tile", type=int, default=None, help="adjoint step kernel variant when it differs")
     ap.add_argument("--plain-shots", type=int, default=2,
                     help="shots of the plain one-shot-per-launch form timed beside the batched one (0: skip)")
     args = ap.parse_args()

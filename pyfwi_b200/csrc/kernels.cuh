@@ -491,51 +491,10 @@ __global__ void __launch_bounds__(NTHREADS) rev_step(const __grid_constant__ Ste
 template <int R, int TZ>
 struct AdjShape {
     static constexpr int W = TX + 4 * R;
-    static constexpr int HT = TZ + 4 * R;  // adjoint velocity + buoyancy rows
-    static constexpr int HV = TZ + 2 * R;  // adjoint stress + lam/mu rows
-    static constexpr int FLOATS = 3 * HT * W + 5 * HV * W;
+    static constexpr int HT = TZ + 4 * R;  // b * adjoint velocity rows
+    static constexpr int HV = TZ + 2 * R;  // adjoint stress rows
+    static constexpr int FLOATS = 2 * HT * W + 3 * HV * W;
 };
-
-// Add the residual of one line to the shared arrays.  Velocity components go
-// to rows [i0-2R, ...) (ht rows), stresses to rows [i0-R, ...) (hv rows).
-template <int R, int TZ>
-__device__ __forceinline__ void inject_line(const AdjArgs &a, int l, int shot, int i0, int sx0, float *s_avx,
-                                            float *s_avz, float *s_atx, float *s_atz, float *s_atxz)
-{
-    using S = AdjShape<R, TZ>;
-    constexpr int W = S::W, HT = S::HT, HV = S::HV;
-    const Lines &L = a.lines;
-    // receivers of this line inside the shared window, one per thread
-    int lo, hi;  // k range
-    if (L.drow[l] == 0) {
-        int rr = L.row0[l] - (i0 - 2 * R);
-        if (rr < 0 || rr >= HT) return;
-        int d0 = sx0 - L.col0[l], d1 = sx0 + W - 1 - L.col0[l];
-        lo = d0 <= 0 ? 0 : (d0 + L.dcol[l] - 1) / L.dcol[l];
-        hi = d1 < 0 ? -1 : d1 / L.dcol[l];
-    } else {
-        int cc = L.col0[l] - sx0;
-        if (cc < 0 || cc >= W) return;
-        int d0 = (i0 - 2 * R) - L.row0[l], d1 = (i0 - 2 * R) + HT - 1 - L.row0[l];
-        lo = d0 <= 0 ? 0 : (d0 + L.drow[l] - 1) / L.drow[l];
-        hi = d1 < 0 ? -1 : d1 / L.drow[l];
-    }
-    if (hi > L.count[l] - 1) hi = L.count[l] - 1;
-    for (int k = lo + (int)threadIdx.x; k <= hi; k += NTHREADS) {
-        int i = L.row0[l] + k * L.drow[l], j = L.col0[l] + k * L.dcol[l];
-        if (i < 0 || i >= a.g.tnz || j < 0 || j >= a.g.tnx) continue;
-        long long o = (long long)a.inj_row * a.ns * a.nr + (long long)shot * a.nr + L.slot0[l] + k;
-        int cc = j - sx0;
-        int rt = i - (i0 - 2 * R), rv = i - (i0 - R);
-        if (a.res[0]) s_avx[rt * W + cc] += __ldg(a.res[0] + o);
-        if (a.res[1]) s_avz[rt * W + cc] += __ldg(a.res[1] + o);
-        if (rv >= 0 && rv < HV) {
-            if (a.res[2]) s_atx[rv * W + cc] += __ldg(a.res[2] + o);
-            if (a.res[3]) s_atz[rv * W + cc] += __ldg(a.res[3] + o);
-            if (a.res[4]) s_atxz[rv * W + cc] += __ldg(a.res[4] + o);
-        }
-    }
-}
 
 __device__ __forceinline__ float bf(const __nv_bfloat16 *p, long long i) { return __bfloat162float(p[i]); }
 
@@ -546,12 +505,17 @@ __global__ void __launch_bounds__(NTHREADS) adj_step(const __grid_constant__ Adj
     constexpr int W = S::W, HT = S::HT, HV = S::HV, VW = TX + 2 * R;
     extern __shared__ float4 smem4[];
     float *sm = reinterpret_cast<float *>(smem4);
-    float *s_avx = sm, *s_avz = s_avx + HT * W, *s_b = s_avz + HT * W;
-    float *s_atx = s_b + HT * W, *s_atz = s_atx + HV * W, *s_atxz = s_atz + HV * W;
-    float *s_lam = s_atxz + HV * W, *s_mu = s_lam + HV * W;
+    // rows i0-2R ..: b*Avx and b*Avz (the operands of the adjoint stress
+    // differences); after the stress update they hold lam*Atx and
+    // (lam+2mu)*Atz on rows i0-R ..
+    float *s_pvx = sm, *s_pvz = s_pvx + HT * W;
+    // rows i0-R ..: Atx, Atz, Atxz; after the stress update (lam+2mu)*Atx,
+    // lam*Atz, mu*Atxz (the operands of the adjoint velocity differences)
+    float *s_atx = s_pvz + HT * W, *s_atz = s_atx + HV * W, *s_atxz = s_atz + HV * W;
 
     const Grid &g = a.g;
-    const int slot = blockIdx.z, shot = a.shot0 + slot;
+    const long long P = g.plane;
+    const int slot = blockIdx.z;
     const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TZ, sx0 = j0 - 2 * R;
     const float *in = a.in + slot * a.in_stride;
     float *out = a.out + slot * a.out_stride;
@@ -561,42 +525,62 @@ __global__ void __launch_bounds__(NTHREADS) adj_step(const __grid_constant__ Adj
     for (int e = tid; e < HT * (W / 4); e += NTHREADS) {
         int r = e / (W / 4), q = e - r * (W / 4);
         int gi = i0 - 2 * R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
-        st4s(s_avx + o, ld4(in + VX * g.plane, g, gi, gj));
-        st4s(s_avz + o, ld4(in + VZ * g.plane, g, gi, gj));
-        st4s(s_b + o, ld4(a.mat + 2 * g.plane, g, gi, gj));
+        const float4 b = ld4(a.mat + 2 * P, g, gi, gj), vx = ld4(in + VX * P, g, gi, gj),
+                     vz = ld4(in + VZ * P, g, gi, gj);
+        st4s(s_pvx + o, make_float4(vx.x * b.x, vx.y * b.y, vx.z * b.z, vx.w * b.w));
+        st4s(s_pvz + o, make_float4(vz.x * b.x, vz.y * b.y, vz.z * b.z, vz.w * b.w));
     }
     for (int e = tid; e < HV * (W / 4); e += NTHREADS) {
         int r = e / (W / 4), q = e - r * (W / 4);
         int gi = i0 - R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
-        st4s(s_atx + o, ld4(in + TXX * g.plane, g, gi, gj));
-        st4s(s_atz + o, ld4(in + TZZ * g.plane, g, gi, gj));
-        st4s(s_atxz + o, ld4(in + TXZ * g.plane, g, gi, gj));
-        st4s(s_lam + o, ld4(a.mat, g, gi, gj));
-        st4s(s_mu + o, ld4(a.mat + g.plane, g, gi, gj));
+        st4s(s_atx + o, ld4(in + TXX * P, g, gi, gj));
+        st4s(s_atz + o, ld4(in + TZZ * P, g, gi, gj));
+        st4s(s_atxz + o, ld4(in + TXZ * P, g, gi, gj));
     }
     __syncthreads();
-    if (a.inj_row >= 0) {
-        for (int l = 0; l < a.lines.n; ++l) {
-            inject_line<R, TZ>(a, l, shot, i0, sx0, s_avx, s_avz, s_atx, s_atz, s_atxz);
-            __syncthreads();
-        }
-    }
 
-    // adjoint stresses on the tile plus an R-cell ring (Adj_update_tau)
+    // adjoint stresses on the tile plus an R-cell ring (Adj_update_tau); the
+    // tile's own cells go straight to the output
     for (int e = tid; e < HV * VW; e += NTHREADS) {
         int r = e / VW, cc = e - r * VW;
         int gi = i0 - R + r, gj = j0 - R + cc;
-        if (!in_domain(g, R, gi, gj)) continue;
         int is = r * W + cc + R, iv = is + R * W;
-        float dx = __ldg(a.dampx + gj + XO), dz = __ldg(a.dampz + gi + ZO);
+        const bool tile = r >= R && r < R + TZ && cc >= R && cc < R + TX && gi < g.tnz && gj < g.tnx;
         float atx = s_atx[is], atz = s_atz[is], atxz = s_atxz[is];
-        atx = atx + (-dt) * (dx * atx + dfwd_p<R>(s_avx, s_b, iv, 1, a.k.cx));
-        atz = atz + (-dt) * (dz * atz + dbwd_p<R>(s_avz, s_b, iv, W, a.k.cz));
-        atxz = atxz + (-dt) * ((dx + dz) * atxz +
-                               (dfwd_p<R>(s_avx, s_b, iv, W, a.k.cz) + dbwd_p<R>(s_avz, s_b, iv, 1, a.k.cx)));
-        s_atx[is] = atx;
-        s_atz[is] = atz;
-        s_atxz[is] = atxz;
+        if (in_domain(g, R, gi, gj)) {
+            float dx = __ldg(a.dampx + gj + XO), dz = __ldg(a.dampz + gi + ZO);
+            atx = atx + (-dt) * (dx * atx + dfwd<R>(s_pvx, iv, 1, a.k.cx));
+            atz = atz + (-dt) * (dz * atz + dbwd<R>(s_pvz, iv, W, a.k.cz));
+            atxz = atxz + (-dt) * ((dx + dz) * atxz + (dfwd<R>(s_pvx, iv, W, a.k.cz) + dbwd<R>(s_pvz, iv, 1, a.k.cx)));
+            s_atx[is] = atx;
+            s_atz[is] = atz;
+            s_atxz[is] = atxz;
+        }
+        if (tile) {
+            const long long co = cell_off(g, gi, gj);
+            out[TXX * P + co] = atx;
+            out[TZZ * P + co] = atz;
+            out[TXZ * P + co] = atxz;
+        }
+    }
+    __syncthreads();
+
+    // material products of the new adjoint stresses
+    for (int e = tid; e < HV * VW; e += NTHREADS) {
+        int r = e / VW, cc = e - r * VW;
+        int gi = i0 - R + r, gj = j0 - R + cc;
+        int is = r * W + cc + R;
+        // lam = mu = 0 in the zero frame and beyond the allocated rows / columns
+        const bool alloc = gi + ZO >= 0 && gi + ZO < g.rows && gj + XO >= 0 && gj + XO < g.pitch;
+        const long long co = alloc ? cell_off(g, gi, gj) : 0;
+        const float lam = alloc ? __ldg(a.mat + co) : 0.f, mu = alloc ? __ldg(a.mat + P + co) : 0.f;
+        const float l2m = lam + 2.f * mu;
+        const float atx = s_atx[is], atz = s_atz[is], atxz = s_atxz[is];
+        s_atx[is] = l2m * atx;
+        s_atz[is] = lam * atz;
+        s_atxz[is] = mu * atxz;
+        s_pvx[is] = lam * atx;
+        s_pvz[is] = l2m * atz;
     }
     __syncthreads();
 
@@ -611,27 +595,23 @@ __global__ void __launch_bounds__(NTHREADS) adj_step(const __grid_constant__ Adj
     for (int r = tid / TX; r < TZ; r += NTHREADS / TX) {
         int gi = i0 + r;
         if (gi >= g.tnz) break;
-        int is = (r + R) * W + c + 2 * R, iv = is + R * W;
-        float avx = s_avx[iv], avz = s_avz[iv];
+        int is = (r + R) * W + c + 2 * R;
         long long co = cell_off(g, gi, gj);
+        float avx = __ldg(in + VX * P + co), avz = __ldg(in + VZ * P + co);
         if (in_domain(g, R, gi, gj)) {
             float dx = __ldg(a.dampx + gj + XO), dz = __ldg(a.dampz + gi + ZO);
-            float sx = dbwd_l2m<R>(s_lam, s_mu, s_atx, is, 1, a.k.cx) + dbwd_p<R>(s_lam, s_atz, is, 1, a.k.cx) +
-                       dbwd_p<R>(s_mu, s_atxz, is, W, a.k.cz);
-            float sz = dfwd_p<R>(s_lam, s_atx, is, W, a.k.cz) + dfwd_l2m<R>(s_lam, s_mu, s_atz, is, W, a.k.cz) +
-                       dfwd_p<R>(s_mu, s_atxz, is, 1, a.k.cx);
+            float sx = dbwd<R>(s_atx, is, 1, a.k.cx) + dbwd<R>(s_atz, is, 1, a.k.cx) + dbwd<R>(s_atxz, is, W, a.k.cz);
+            float sz = dfwd<R>(s_pvx, is, W, a.k.cz) + dfwd<R>(s_pvz, is, W, a.k.cz) + dfwd<R>(s_atxz, is, 1, a.k.cx);
             avx = avx + (-dt) * ((2.f * dx + dz) * avx + sx);
             avz = avz + (-dt) * ((dx + 2.f * dz) * avz + sz);
         }
-        float atx = s_atx[is], atz = s_atz[is], atxz = s_atxz[is];
-        out[VX * g.plane + co] = avx;
-        out[VZ * g.plane + co] = avz;
-        out[TXX * g.plane + co] = atx;
-        out[TZZ * g.plane + co] = atz;
-        out[TXZ * g.plane + co] = atxz;
+        out[VX * P + co] = avx;
+        out[VZ * P + co] = avz;
 
         if (gi < glo || gi > g.tnz - R - a.npml || gj < glo || gj > g.tnx - R - a.npml) continue;
-        const long long P = g.plane, sz_ = g.pitch;
+        const long long sz_ = g.pitch;
+        // the new adjoint stresses this CTA wrote above (plain loads: written in this kernel)
+        const float atx = out[TXX * P + co], atz = out[TZZ * P + co], atxz = out[TXZ * P + co];
         float dzp_vx, dxm_vz, dxp_vx, dzm_vz, dzp_tz, dxm_tx, dxp_txz, dzm_txz;
         float vx = 0.f, vz = 0.f, tx = 0.f, tz = 0.f, txz = 0.f;
         if (F) {
@@ -684,7 +664,7 @@ __global__ void __launch_bounds__(NTHREADS) adj_step(const __grid_constant__ Adj
 #undef BFWD
 #undef BBWD
         }
-        float b = s_b[iv];
+        const float b = __ldg(a.mat + 2 * P + co);
         float gmu = G[0 * P + co], glam = G[1 * P + co], grho = G[2 * P + co];
         gmu += 2.f * dt * (atx * dxp_vx + atz * dzm_vz) + dt * atxz * (dzp_vx + dxm_vz);
         glam += dt * (atx + atz) * (dxp_vx + dzm_vz);

@@ -162,9 +162,25 @@ int launch_fwd(pyfwi_plan *p, const StepArgs &a, int nslots, cudaStream_t s, boo
     return PYFWI_OK;
 }
 
+// Adds the residual row of this step to the input adjoint state, in place
+// (Adj_injSrc, elastic_surface.cl:48-71), before the step kernel reads it.
+int launch_inject(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
+{
+    if (a.inj_row < 0) return PYFWI_OK;
+    // one CTA per shot: receivers of different lines on one cell then add in line order
+    inject_kernel<<<dim3(1, nslots), 256, 0, s>>>(p->g, const_cast<float *>(a.in), a.in_stride, a.shot0, a.inj_row,
+                                                  a.res[0], a.res[1], a.res[2], a.res[3], a.res[4], p->lines, a.ns,
+                                                  a.nr, 0);
+    p->launches++;
+    CKL();
+    return PYFWI_OK;
+}
+
 template <int R, int TZ, bool E>
 int launch_adj_t(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
 {
+    int rc = launch_inject(p, a, nslots, s);
+    if (rc) return rc;
     dim3 grid((p->g.tnx + TX - 1) / TX, (p->g.tnz + TZ - 1) / TZ, nslots);
     size_t sm = AdjShape<R, TZ>::FLOATS * sizeof(float);
     static bool attr = false;
@@ -282,18 +298,12 @@ template <int R, int W, bool E>
 int launch_adj_stream_t(pyfwi_plan *p, AdjArgs a, int nslots, cudaStream_t s, const float *ws)
 {
     using S = AdjRing<R, W, ADJ_PF, E>;
-    if (a.inj_row >= 0) {  // the streaming adjoint reads the residual from its input state
-        // one CTA per shot: receivers of different lines on one cell then add in line order
-        dim3 ig(1, nslots);
-        inject_kernel<<<ig, 256, 0, s>>>(p->g, const_cast<float *>(a.in), a.in_stride, a.shot0, a.inj_row,
-                                         a.res[0], a.res[1], a.res[2], a.res[3], a.res[4], p->lines, a.ns, a.nr, 0);
-        p->launches++;
-        CKL();
-    }
+    int rc = launch_inject(p, a, nslots, s);
+    if (rc) return rc;
     a.chunk = stream_chunk(p, nslots, S::T);
     a.tbase = ws;
     a.err = reinterpret_cast<int *>(const_cast<char *>(reinterpret_cast<const char *>(ws)) + ERR_OFF);
-    int rc = workspace_map(p, ws, W, &a.tmap);
+    rc = workspace_map(p, ws, W, &a.tmap);
     if (rc) return rc;
     const int iw = S::T - 2 * R;
     dim3 grid((p->g.tnx + iw - 1) / iw, (p->g.tnz + a.chunk - 1) / a.chunk, nslots);

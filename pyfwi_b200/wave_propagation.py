@@ -269,7 +269,8 @@ class WavePreparation:
             o.segment = int(seg)
             o.snapshot = snapshot
             o.shot_batch = int(batch)
-            o.energy = 1 if self.energy_balancing else 0
+            # the exact gradient is not preconditioned: no energy terms
+            o.energy = 1 if self.energy_balancing and self.adjoint != "exact" else 0
             o.tile, o.adj_tile = variants
             o.adjoint = N.ADJOINT_EXACT if self.adjoint == "exact" else N.ADJOINT_REFERENCE
             o.graph = int(bool(inpa.get("graph", False)))
@@ -282,8 +283,8 @@ class WavePreparation:
         self.adjoint = inpa.get("adjoint", "reference")
         if self.adjoint not in ("reference", "exact"):
             raise ValueError("inpa['adjoint'] must be 'reference' or 'exact'")
-        if self.adjoint == "exact" and (mode != "exact" or self.energy_balancing):
-            raise ValueError("inpa['adjoint'] = 'exact' needs checkpoint 'exact' and no energy balancing")
+        if self.adjoint == "exact" and mode != "exact":
+            raise ValueError("inpa['adjoint'] = 'exact' needs checkpoint 'exact'")
         snap = inpa.get("snapshot", "fp32")
         if snap not in ("fp32", "bf16") or (snap == "bf16" and mode != "exact"):
             raise ValueError("inpa['snapshot'] must be 'fp32' or 'bf16' (bf16 with checkpoint 'exact' only)")

@@ -45,12 +45,13 @@ def l2_residual_np(d_est, d_obs):
     return {k: np.float32(pe[k] - po[k]) for k in O.FIELDS}
 
 
-def fp64_propagator(case):
-    """The FP64 oracle propagator of a case, storing every step (chpr 100)."""
+def fp64_propagator(case, precision="fp64"):
+    """The oracle propagator of a case (FP64 unless asked), storing every
+    step (chpr 100)."""
     import oracle as O
     inpa = case["inpa"]
     src = O.Ricker(case["src_loc"], inpa["dh"], inpa["dt"], case["src_type"])
     src.Ricker(case["fdom"])
     return O.OracleWavePropagator(inpa, src, case["rec_loc"], case["model_est"]["vp"].shape,
                                   components=case["components"], n_well_rec=case["n_well_rec"], chpr=100,
-                                  precision="fp64")
+                                  precision=precision)

@@ -147,7 +147,7 @@ def test_autotuned_variants():
     for k, v in d.items():
         assert rel_l2(v, g["d_est_" + k]) < SEIS_TOL, k
     res = l2_residual_np(_golden_section(g, "d_est_"), _golden_section(g, "d_obs_"))
-    grad = W.gradient(res, parameterization="lmd")
+    grad = W.gradient(res, parameterization=case["param"])
     for k, v in grad.items():
         assert rel_l2(v, g["grad_" + k]) < GRAD_TOL, k
 
