@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PYFWI_ABI_VERSION 3
+#define PYFWI_ABI_VERSION 4
 
 enum pyfwi_status {
     PYFWI_OK = 0,
@@ -167,6 +167,28 @@ int pyfwi_gradient(pyfwi_plan *plan, void *workspace, size_t workspace_bytes, co
 /* L2 misfit and residual (CostFunction.l2, fwi_tools.py:1402-1422):
  * res = est - obs (float32), *misfit += 0.5 * sum(res^2) (float64 sum on device). */
 int pyfwi_l2_residual(const float *est, const float *obs, float *res, int64_t n, double *misfit, void *stream);
+
+/* One misfit-and-gradient evaluation, the work of FWI.fprime (fwi.py:
+ * 229-246: forward_modeling, CostFunction.l2 on the section, gradient) fused
+ * per shot group: each group is modelled once, its L2 residual against the
+ * observed traces is formed on the device, and its adjoint runs while its
+ * forward states are still stored.  pyfwi_set_model must come first.
+ * observed[5]: device [nt_ext][ns*nr] observed traces per field in the
+ *   '2d' section layout, NULL for a field not in the misfit.  mean_stress = 1
+ *   for components 0: the txx and tzz slots then hold the observed 'taux' and
+ *   'tauz' sections, both compared with (txx + tzz) / 2.
+ * adjoint_source[5]: device [nt_ext][ns*nr] buffers receiving the adjoint
+ *   sources (the section residuals; for PYFWI_ADJOINT_EXACT with
+ *   mean_stress, half their sum in both stress slots); needed where observed
+ *   is set (both stress slots with mean_stress).
+ * traces: device [5][nt_ext][ns*nr], receives the modelled traces.
+ * misfit: device double, receives sum over the section keys of
+ *   0.5 * |modelled - observed|^2 (accumulated in double).
+ * Not for surveys whose section reorders traces (acquisition 2 with well
+ * receivers): use pyfwi_forward + pyfwi_gradient there. */
+int pyfwi_misfit_gradient(pyfwi_plan *plan, void *workspace, size_t bytes, const float *src_vals, int32_t n_src,
+                          const float *const *observed, int32_t mean_stress, float *const *adjoint_source,
+                          int32_t parameterization, float *traces, float *grad, double *misfit, void *stream);
 
 /* Trace section (acquisition.py:313-333): out = (a + b) / 2 elementwise. */
 int pyfwi_mean2(const float *a, const float *b, float *out, int64_t n, void *stream);

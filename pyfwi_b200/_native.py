@@ -30,7 +30,7 @@ class Geometry(ctypes.Structure):
                 ("mask_row0", _i32), ("mask_row1", _i32), ("mask_col0", _i32), ("mask_col1", _i32)]
 
 
-ABI_VERSION = 3  # PYFWI_ABI_VERSION of include/pyfwi_b200.h
+ABI_VERSION = 4  # PYFWI_ABI_VERSION of include/pyfwi_b200.h
 
 
 class Options(ctypes.Structure):
@@ -64,6 +64,8 @@ def lib():
     L.pyfwi_gradient.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(_P), _i32, _P, _P, _P]
     L.pyfwi_l2_residual.argtypes = [_P, _P, _P, ctypes.c_int64, _P, _P]
     L.pyfwi_mean2.argtypes = [_P, _P, _P, ctypes.c_int64, _P]
+    L.pyfwi_misfit_gradient.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_float), _i32,
+                                        ctypes.POINTER(_P), _i32, ctypes.POINTER(_P), _i32, _P, _P, _P, _P]
     L.pyfwi_smooth.argtypes = [_P, _P, _P, _i32, _i32, _i32, ctypes.POINTER(ctypes.c_double), _i32, _P]
     L.pyfwi_tile_count.argtypes = [_i32]
     L.pyfwi_launch_count.argtypes = [_P, ctypes.POINTER(ctypes.c_int64)]
@@ -79,7 +81,7 @@ def lib():
     for name in ("pyfwi_plan_create", "pyfwi_plan_destroy", "pyfwi_workspace_size", "pyfwi_set_model",
                  "pyfwi_forward", "pyfwi_gradient", "pyfwi_l2_residual", "pyfwi_mean2", "pyfwi_tile_count",
                  "pyfwi_launch_count", "pyfwi_profile_enable", "pyfwi_profile_read", "pyfwi_device_error",
-                 "pyfwi_smooth"):
+                 "pyfwi_smooth", "pyfwi_misfit_gradient"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -65,6 +65,20 @@ __device__ __forceinline__ float4 ld4(const float *plane, const Grid &g, int gi,
 
 __device__ __forceinline__ void st4s(float *s, float4 v) { *reinterpret_cast<float4 *>(s) = v; }
 
+// Asynchronous 16-byte copy of the 4 cells (gi, gj .. gj+3) of `plane` into
+// shared memory (cp.async, bypassing L1), zero-filled where ld4 reads zero.
+__device__ __forceinline__ void cp4(float *dst, const float *plane, const Grid &g, int gi, int gj)
+{
+    const int ar = gi + ZO, ac = gj + XO;
+    const bool ok = ar >= 0 && ar < g.rows && ac >= 0 && ac + 3 < g.pitch;
+    const float *src = ok ? plane + (long long)ar * g.pitch + ac : plane;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(ok ? 16 : 0)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // ---- staggered one-sided differences on a shared-memory array -------------
 // fwd: c1(f[+1]-f[0]) + c2(f[+2]-f[-1]) [+ c3(f[+3]-f[-2]) + c4(f[+4]-f[-3])]
 // bwd: c1(f[0]-f[-1]) + c2(f[+1]-f[-2]) [+ c3(f[+2]-f[-3]) + c4(f[+3]-f[-4])]
@@ -233,6 +247,7 @@ struct AdjArgs {
     int npml;
     int shot0;
     int inj_row;           // residual row injected this step, -1 for none
+    int epi_row;           // tile kernel: residual row the next step injects, added to this step's output (-1: none)
     const float *res[5];   // [nt_ext][ns*nr] residual components (nullable)
     int nr, ns;
     Lines lines;
@@ -245,6 +260,22 @@ struct AdjArgs {
 __device__ __forceinline__ bool in_domain(const Grid &g, int R, int i, int j)
 {
     return i >= R && i <= g.tnz - R && j >= R && j <= g.tnx - R;
+}
+
+// Trace slot k of line l at cell (i, j), or -1 when no receiver of the line sits there.
+__device__ __forceinline__ int line_slot(const Lines &L, int l, int i, int j)
+{
+    int d;
+    if (L.drow[l] == 0) {
+        d = j - L.col0[l];
+        if (i != L.row0[l] || d < 0 || d % L.dcol[l]) return -1;
+        d /= L.dcol[l];
+    } else {
+        d = i - L.row0[l];
+        if (j != L.col0[l] || d < 0 || d % L.drow[l]) return -1;
+        d /= L.drow[l];
+    }
+    return d < L.count[l] ? d : -1;
 }
 
 // Record the five fields of `st` at cell (i, j) into every trace slot whose
@@ -280,110 +311,274 @@ __device__ __forceinline__ void record_cell(const StepArgs &a, const float *st, 
 // ---------------------------------------------------------------------------
 template <int R, int TZ>
 struct FwdShape {
-    static constexpr int W = TX + 4 * R;   // shared row width
-    static constexpr int HT = TZ + 4 * R;  // stress rows (tile + 2R halo)
-    static constexpr int HV = TZ + 2 * R;  // velocity rows (tile + R halo)
-    static constexpr int FLOATS = 3 * HT * W + 3 * HV * W;
+    // Each thread updates 4 adjacent columns of one row from aligned float4
+    // shared-memory loads, keeping the x-neighbours in registers.
+    static constexpr int SW = TX + 16;     // stress row width: columns j0-8 .. j0+TX+7
+    static constexpr int VW = TX + 8;      // velocity row width: columns j0-4 .. j0+TX+3
+    static constexpr int HT = TZ + 4 * R;  // stress rows i0-2R ..
+    static constexpr int HV = TZ + 2 * R;  // velocity rows i0-R ..
+    static constexpr int FLOATS = 3 * HT * SW + 3 * HV * VW + 2 * TZ * TX;
+    static_assert(R <= 4, "x halo of 4 columns per group");
 };
+
+__device__ __forceinline__ float4 ld4s(const float *s) { return *reinterpret_cast<const float4 *>(s); }
+__device__ __forceinline__ float f4(const float4 &v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+
+// Three aligned float4 of a shared row around column c (c - 4 .. c + 7).
+__device__ __forceinline__ void row12(float (&v)[12], const float *row, int c)
+{
+    const float4 a = ld4s(row + c - 4), b = ld4s(row + c), d = ld4s(row + c + 4);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    v[8] = d.x; v[9] = d.y; v[10] = d.z; v[11] = d.w;
+}
+
+// The differences of dfwd / dbwd, in the same operation order, on registers:
+// x: v[4 + k] is column c + k; z: w[m] (float4 rows centre - R .. centre + R,
+// w[R] the centre), component k.
+template <int R>
+__device__ __forceinline__ float xfwd(const float (&v)[12], int k, const float *c)
+{
+    const int o = 4 + k;
+    float r = c[0] * (v[o + 1] - v[o]);
+    r = fmaf(c[1], v[o + 2] - v[o - 1], r);
+    if (R == 4) {
+        r = fmaf(c[2], v[o + 3] - v[o - 2], r);
+        r = fmaf(c[3], v[o + 4] - v[o - 3], r);
+    }
+    return r;
+}
+
+template <int R>
+__device__ __forceinline__ float xbwd(const float (&v)[12], int k, const float *c)
+{
+    const int o = 4 + k;
+    float r = c[0] * (v[o] - v[o - 1]);
+    r = fmaf(c[1], v[o + 1] - v[o - 2], r);
+    if (R == 4) {
+        r = fmaf(c[2], v[o + 2] - v[o - 3], r);
+        r = fmaf(c[3], v[o + 3] - v[o - 4], r);
+    }
+    return r;
+}
+
+template <int R>
+__device__ __forceinline__ float zfwd(const float4 (&w)[2 * R + 1], int k, const float *c)
+{
+    float r = c[0] * (f4(w[R + 1], k) - f4(w[R], k));
+    r = fmaf(c[1], f4(w[R + 2], k) - f4(w[R - 1], k), r);
+    if (R == 4) {
+        r = fmaf(c[2], f4(w[R + 3], k) - f4(w[R - 2], k), r);
+        r = fmaf(c[3], f4(w[R + 4], k) - f4(w[R - 3], k), r);
+    }
+    return r;
+}
+
+template <int R>
+__device__ __forceinline__ float zbwd(const float4 (&w)[2 * R + 1], int k, const float *c)
+{
+    float r = c[0] * (f4(w[R], k) - f4(w[R - 1], k));
+    r = fmaf(c[1], f4(w[R + 1], k) - f4(w[R - 2], k), r);
+    if (R == 4) {
+        r = fmaf(c[2], f4(w[R + 2], k) - f4(w[R - 3], k), r);
+        r = fmaf(c[3], f4(w[R + 3], k) - f4(w[R - 4], k), r);
+    }
+    return r;
+}
+
+// Rows centre - R .. centre + R of a shared plane at column c.
+template <int R>
+__device__ __forceinline__ void col_rows(float4 (&w)[2 * R + 1], const float *plane, int width, int centre, int c)
+{
+#pragma unroll
+    for (int m = 0; m <= 2 * R; ++m) w[m] = ld4s(plane + (centre - R + m) * width + c);
+}
+
+// Damping of 4 columns from j (j a multiple of 4), zero outside the allocation.
+__device__ __forceinline__ float4 damp4(const float *dampx, const Grid &g, int j)
+{
+    const int c = j + XO;
+    if (c >= 0 && c + 3 < g.pitch) return __ldg(reinterpret_cast<const float4 *>(dampx + c));
+    float4 v;
+    v.x = (c >= 0 && c < g.pitch) ? __ldg(dampx + c) : 0.f;
+    v.y = (c + 1 >= 0 && c + 1 < g.pitch) ? __ldg(dampx + c + 1) : 0.f;
+    v.z = (c + 2 >= 0 && c + 2 < g.pitch) ? __ldg(dampx + c + 2) : 0.f;
+    v.w = (c + 3 >= 0 && c + 3 < g.pitch) ? __ldg(dampx + c + 3) : 0.f;
+    return v;
+}
 
 template <int R, int TZ>
 __global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ StepArgs a)
 {
     using S = FwdShape<R, TZ>;
-    constexpr int W = S::W, HT = S::HT, HV = S::HV, VW = TX + 2 * R;
+    constexpr int SW = S::SW, VW = S::VW, HT = S::HT, HV = S::HV;
     extern __shared__ float4 smem4[];
     float *sm = reinterpret_cast<float *>(smem4);
-    float *s_txx = sm, *s_tzz = s_txx + HT * W, *s_txz = s_tzz + HT * W;
-    float *s_vx = s_txz + HT * W, *s_vz = s_vx + HV * W, *s_b = s_vz + HV * W;
+    float *s_txx = sm, *s_tzz = s_txx + HT * SW, *s_txz = s_tzz + HT * SW;
+    float *s_vx = s_txz + HT * SW, *s_vz = s_vx + HV * VW, *s_b = s_vz + HV * VW;
+    float *s_lam = s_b + HV * VW, *s_mu = s_lam + TZ * TX;  // the tile's cells
 
     const Grid &g = a.g;
+    const long long P = g.plane;
     const int slot = blockIdx.z, shot = a.shot0 + slot;
-    const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TZ, sx0 = j0 - 2 * R;
+    const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TZ;
     const float *in = a.in + slot * a.in_stride;
     float *out = a.out + slot * a.out_stride;
     const int tid = threadIdx.x;
     const float dt = a.k.dt;
 
-    for (int e = tid; e < HT * (W / 4); e += NTHREADS) {
-        int r = e / (W / 4), q = e - r * (W / 4);
-        int gi = i0 - 2 * R + r, gj = sx0 + 4 * q;
-        int o = r * W + 4 * q;
-        st4s(s_txx + o, ld4(in + TXX * g.plane, g, gi, gj));
-        st4s(s_tzz + o, ld4(in + TZZ * g.plane, g, gi, gj));
-        st4s(s_txz + o, ld4(in + TXZ * g.plane, g, gi, gj));
+    // every copy of the tile in flight at once, then one wait
+    for (int e = tid; e < HT * (SW / 4); e += NTHREADS) {
+        int r = e / (SW / 4), q = e - r * (SW / 4);
+        int gi = i0 - 2 * R + r, gj = j0 - 8 + 4 * q, o = r * SW + 4 * q;
+        cp4(s_txx + o, in + TXX * P, g, gi, gj);
+        cp4(s_tzz + o, in + TZZ * P, g, gi, gj);
+        cp4(s_txz + o, in + TXZ * P, g, gi, gj);
     }
-    for (int e = tid; e < HV * (W / 4); e += NTHREADS) {
-        int r = e / (W / 4), q = e - r * (W / 4);
-        int gi = i0 - R + r, gj = sx0 + 4 * q;
-        int o = r * W + 4 * q;
-        st4s(s_vx + o, ld4(in + VX * g.plane, g, gi, gj));
-        st4s(s_vz + o, ld4(in + VZ * g.plane, g, gi, gj));
-        st4s(s_b + o, ld4(a.mat + 2 * g.plane, g, gi, gj));
+    for (int e = tid; e < HV * (VW / 4); e += NTHREADS) {
+        int r = e / (VW / 4), q = e - r * (VW / 4);
+        int gi = i0 - R + r, gj = j0 - 4 + 4 * q, o = r * VW + 4 * q;
+        cp4(s_vx + o, in + VX * P, g, gi, gj);
+        cp4(s_vz + o, in + VZ * P, g, gi, gj);
+        cp4(s_b + o, a.mat + 2 * P, g, gi, gj);
     }
+    for (int e = tid; e < TZ * (TX / 4); e += NTHREADS) {
+        int r = e / (TX / 4), q = e - r * (TX / 4), o = r * TX + 4 * q;
+        cp4(s_lam + o, a.mat, g, i0 + r, j0 + 4 * q);
+        cp4(s_mu + o, a.mat + P, g, i0 + r, j0 + 4 * q);
+    }
+    cp_wait_all();
     __syncthreads();
     if (a.add_src && tid == 0) {  // wave_propagation.py:652-664, elastic_surface.cl:23-28
-        int si = a.srcz[shot], sj = a.srcx[shot], c = sj - sx0;
-        if (c >= 0 && c < W) {
-            int rt = si - (i0 - 2 * R), rv = si - (i0 - R);
-            if (rt >= 0 && rt < HT) {
-                s_txx[rt * W + c] += a.src.z;
-                s_tzz[rt * W + c] += a.src.w;
-            }
-            if (rv >= 0 && rv < HV) {
-                s_vx[rv * W + c] += a.src.x;
-                s_vz[rv * W + c] += a.src.y;
-            }
+        const int si = a.srcz[shot], sj = a.srcx[shot];
+        const int ct = sj - (j0 - 8), cv = sj - (j0 - 4), rt = si - (i0 - 2 * R), rv = si - (i0 - R);
+        if (ct >= 0 && ct < SW && rt >= 0 && rt < HT) {
+            s_txx[rt * SW + ct] += a.src.z;
+            s_tzz[rt * SW + ct] += a.src.w;
+        }
+        if (cv >= 0 && cv < VW && rv >= 0 && rv < HV) {
+            s_vx[rv * VW + cv] += a.src.x;
+            s_vz[rv * VW + cv] += a.src.y;
         }
     }
     __syncthreads();
 
-    // velocities on the tile plus an R-cell ring (update_velx / update_velz)
-    for (int e = tid; e < HV * VW; e += NTHREADS) {
-        int r = e / VW, cc = e - r * VW;
-        int gi = i0 - R + r, gj = j0 - R + cc;
-        if (!in_domain(g, R, gi, gj)) continue;  // outside: keeps its value
-        int iv = r * W + cc + R, it = iv + R * W;
-        float d = __ldg(a.dampx + gj + XO) + __ldg(a.dampz + gi + ZO);
-        float b = s_b[iv];
-        float vx = s_vx[iv] + dt * (b * (dbwd<R>(s_txx, it, 1, a.k.cx) + dbwd<R>(s_txz, it, W, a.k.cz)));
-        vx = vx + dt * (-d * vx);
-        float vz = s_vz[iv] + dt * (b * (dfwd<R>(s_tzz, it, W, a.k.cz) + dfwd<R>(s_txz, it, 1, a.k.cx)));
-        vz = vz + dt * (-d * vz);
-        s_vx[iv] = vx;
-        s_vz[iv] = vz;
+    // velocities (update_velx / update_velz) on rows i0-R .. and columns
+    // j0-4 .., 4 columns per thread
+    for (int e = tid; e < HV * (VW / 4); e += NTHREADS) {
+        const int r = e / (VW / 4), q = e - r * (VW / 4);
+        const int gi = i0 - R + r, gj = j0 - 4 + 4 * q;
+        const int rt = r + R, ct = 4 * q + 4, o = r * VW + 4 * q;
+        float4 vx = ld4s(s_vx + o), vz = ld4s(s_vz + o);
+        const float4 b = ld4s(s_b + o), dx = damp4(a.dampx, g, gj);
+        const float dz = (gi + ZO >= 0 && gi + ZO < g.rows) ? __ldg(a.dampz + gi + ZO) : 0.f;
+        float t[12];
+        float4 w[2 * R + 1];
+        float rx[4], rz[4];
+        row12(t, s_txx + rt * SW, ct);  // Dx- txx
+#pragma unroll
+        for (int k = 0; k < 4; ++k) rx[k] = xbwd<R>(t, k, a.k.cx);
+        col_rows<R>(w, s_txz, SW, rt, ct);  // Dz- txz
+#pragma unroll
+        for (int k = 0; k < 4; ++k) rz[k] = zbwd<R>(w, k, a.k.cz);
+        float nvx[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float v = f4(vx, k);
+            if (in_domain(g, R, gi, gj + k)) {
+                const float d = f4(dx, k) + dz;
+                v = v + dt * (f4(b, k) * (rx[k] + rz[k]));
+                v = v + dt * (-d * v);
+            }
+            nvx[k] = v;
+        }
+        row12(t, s_txz + rt * SW, ct);  // Dx+ txz
+#pragma unroll
+        for (int k = 0; k < 4; ++k) rx[k] = xfwd<R>(t, k, a.k.cx);
+        col_rows<R>(w, s_tzz, SW, rt, ct);  // Dz+ tzz
+#pragma unroll
+        for (int k = 0; k < 4; ++k) rz[k] = zfwd<R>(w, k, a.k.cz);
+        float nvz[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float v = f4(vz, k);
+            if (in_domain(g, R, gi, gj + k)) {
+                const float d = f4(dx, k) + dz;
+                v = v + dt * (f4(b, k) * (rz[k] + rx[k]));
+                v = v + dt * (-d * v);
+            }
+            nvz[k] = v;
+        }
+        st4s(s_vx + o, make_float4(nvx[0], nvx[1], nvx[2], nvx[3]));
+        st4s(s_vz + o, make_float4(nvz[0], nvz[1], nvz[2], nvz[3]));
     }
     __syncthreads();
 
-    // stresses on the tile (update_tauz / update_tauxz), one column per thread
-    const int c = tid % TX;
-    const int gj = j0 + c;
-    if (gj >= g.tnx) return;
-    for (int r = tid / TX; r < TZ; r += NTHREADS / TX) {
-        int gi = i0 + r;
-        if (gi >= g.tnz) break;
-        int iv = (r + R) * W + c + 2 * R, it = iv + R * W;
-        float txx = s_txx[it], tzz = s_tzz[it], txz = s_txz[it];
-        long long co = cell_off(g, gi, gj);
-        if (in_domain(g, R, gi, gj)) {
-            float lam = __ldg(a.mat + co), mu = __ldg(a.mat + g.plane + co);
-            float d = __ldg(a.dampx + gj + XO) + __ldg(a.dampz + gi + ZO);
-            float dxp_vx = dfwd<R>(s_vx, iv, 1, a.k.cx), dzm_vz = dbwd<R>(s_vz, iv, W, a.k.cz);
-            float dxm_vz = dbwd<R>(s_vz, iv, 1, a.k.cx), dzp_vx = dfwd<R>(s_vx, iv, W, a.k.cz);
-            float l2m = lam + 2.f * mu;
-            txx = txx + dt * (l2m * dxp_vx + lam * dzm_vz);
-            tzz = tzz + dt * (l2m * dzm_vz + lam * dxp_vx);
-            txx = txx + dt * (-d * txx);
-            tzz = tzz + dt * (-d * tzz);
-            txz = txz + dt * (mu * (dxm_vz + dzp_vx));
-            txz = txz + dt * (-d * txz);
+    // stresses (update_tauz / update_tauxz) on the tile, 4 columns per thread
+    for (int e = tid; e < TZ * (TX / 4); e += NTHREADS) {
+        const int r = e / (TX / 4), q = e - r * (TX / 4);
+        const int gi = i0 + r, gj = j0 + 4 * q;
+        if (gi >= g.tnz || gj >= g.tnx) continue;
+        const int rv = r + R, cv = 4 * q + 4, rt = r + 2 * R, ct = 4 * q + 8;
+        const long long co = cell_off(g, gi, gj);
+        const float4 vxc = ld4s(s_vx + rv * VW + cv), vzc = ld4s(s_vz + rv * VW + cv);
+        float4 txx = ld4s(s_txx + rt * SW + ct), tzz = ld4s(s_tzz + rt * SW + ct), txz = ld4s(s_txz + rt * SW + ct);
+        const float4 lam = ld4s(s_lam + r * TX + 4 * q), mu = ld4s(s_mu + r * TX + 4 * q),
+                     dx = damp4(a.dampx, g, gj);
+        const float dz = __ldg(a.dampz + gi + ZO);
+        float t[12];
+        float4 w[2 * R + 1];
+        float dxp_vx[4], dzm_vz[4], dxm_vz[4], dzp_vx[4];
+        row12(t, s_vx + rv * VW, cv);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dxp_vx[k] = xfwd<R>(t, k, a.k.cx);
+        row12(t, s_vz + rv * VW, cv);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dxm_vz[k] = xbwd<R>(t, k, a.k.cx);
+        col_rows<R>(w, s_vz, VW, rv, cv);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dzm_vz[k] = zbwd<R>(w, k, a.k.cz);
+        col_rows<R>(w, s_vx, VW, rv, cv);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dzp_vx[k] = zfwd<R>(w, k, a.k.cz);
+        float oxx[4], ozz[4], oxz[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float sxx = f4(txx, k), szz = f4(tzz, k), sxz = f4(txz, k);
+            if (in_domain(g, R, gi, gj + k)) {
+                const float l = f4(lam, k), m = f4(mu, k), d = f4(dx, k) + dz;
+                const float l2m = l + 2.f * m;
+                sxx = sxx + dt * (l2m * dxp_vx[k] + l * dzm_vz[k]);
+                szz = szz + dt * (l2m * dzm_vz[k] + l * dxp_vx[k]);
+                sxx = sxx + dt * (-d * sxx);
+                szz = szz + dt * (-d * szz);
+                sxz = sxz + dt * (m * (dxm_vz[k] + dzp_vx[k]));
+                sxz = sxz + dt * (-d * sxz);
+            }
+            oxx[k] = sxx;
+            ozz[k] = szz;
+            oxz[k] = sxz;
         }
-        out[VX * g.plane + co] = s_vx[iv];
-        out[VZ * g.plane + co] = s_vz[iv];
-        out[TXX * g.plane + co] = txx;
-        out[TZZ * g.plane + co] = tzz;
-        out[TXZ * g.plane + co] = txz;
-        if (a.snap) write_snap(a.snap + slot * a.snap_stride, g.plane, co, s_vx[iv], s_vz[iv], txx, tzz, txz);
-        if (a.rec_row >= 0) record_cell(a, in, shot, gi, gj);
+        if (gj + 3 < g.tnx) {
+            *reinterpret_cast<float4 *>(out + VX * P + co) = vxc;
+            *reinterpret_cast<float4 *>(out + VZ * P + co) = vzc;
+            *reinterpret_cast<float4 *>(out + TXX * P + co) = make_float4(oxx[0], oxx[1], oxx[2], oxx[3]);
+            *reinterpret_cast<float4 *>(out + TZZ * P + co) = make_float4(ozz[0], ozz[1], ozz[2], ozz[3]);
+            *reinterpret_cast<float4 *>(out + TXZ * P + co) = make_float4(oxz[0], oxz[1], oxz[2], oxz[3]);
+        } else {
+            for (int k = 0; k < 4 && gj + k < g.tnx; ++k) {
+                out[VX * P + co + k] = f4(vxc, k);
+                out[VZ * P + co + k] = f4(vzc, k);
+                out[TXX * P + co + k] = oxx[k];
+                out[TZZ * P + co + k] = ozz[k];
+                out[TXZ * P + co + k] = oxz[k];
+            }
+        }
+        for (int k = 0; k < 4 && gj + k < g.tnx; ++k) {
+            if (a.snap)
+                write_snap(a.snap + slot * a.snap_stride, P, co + k, f4(vxc, k), f4(vzc, k), oxx[k], ozz[k], oxz[k]);
+            if (a.rec_row >= 0) record_cell(a, in, shot, gi, gj + k);
+        }
     }
 }
 
@@ -498,6 +693,24 @@ struct AdjShape {
 
 __device__ __forceinline__ float bf(const __nv_bfloat16 *p, long long i) { return __bfloat162float(p[i]); }
 
+// The next step's residual row (AdjArgs.epi_row) added at cell (i, j) of
+// the output: to the adjoint velocities in registers and the stresses in
+// memory, one receiver line after another.
+__device__ __forceinline__ void inject_epilogue(const AdjArgs &a, int slot, int i, int j, long long co, float &avx,
+                                                float &avz, float *out)
+{
+    const long long P = a.g.plane;
+    for (int l = 0; l < a.lines.n; ++l) {
+        const int ks = line_slot(a.lines, l, i, j);
+        if (ks < 0) continue;
+        const long long o = (long long)a.epi_row * a.ns * a.nr + (long long)(a.shot0 + slot) * a.nr + a.lines.slot0[l] + ks;
+        if (a.res[0]) avx += __ldg(a.res[0] + o);
+        if (a.res[1]) avz += __ldg(a.res[1] + o);
+        for (int f = TXX; f <= TXZ; ++f)
+            if (a.res[f]) out[f * P + co] += __ldg(a.res[f] + o);
+    }
+}
+
 template <int R, int TZ, bool ENERGY>
 __global__ void __launch_bounds__(NTHREADS) adj_step(const __grid_constant__ AdjArgs a)
 {
@@ -522,6 +735,15 @@ __global__ void __launch_bounds__(NTHREADS) adj_step(const __grid_constant__ Adj
     const int tid = threadIdx.x;
     const float dt = a.k.dt;
 
+    // the stresses as asynchronous copies, in flight while the velocity
+    // products are loaded and stored
+    for (int e = tid; e < HV * (W / 4); e += NTHREADS) {
+        int r = e / (W / 4), q = e - r * (W / 4);
+        int gi = i0 - R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
+        cp4(s_atx + o, in + TXX * P, g, gi, gj);
+        cp4(s_atz + o, in + TZZ * P, g, gi, gj);
+        cp4(s_atxz + o, in + TXZ * P, g, gi, gj);
+    }
     for (int e = tid; e < HT * (W / 4); e += NTHREADS) {
         int r = e / (W / 4), q = e - r * (W / 4);
         int gi = i0 - 2 * R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
@@ -530,13 +752,7 @@ __global__ void __launch_bounds__(NTHREADS) adj_step(const __grid_constant__ Adj
         st4s(s_pvx + o, make_float4(vx.x * b.x, vx.y * b.y, vx.z * b.z, vx.w * b.w));
         st4s(s_pvz + o, make_float4(vz.x * b.x, vz.y * b.y, vz.z * b.z, vz.w * b.w));
     }
-    for (int e = tid; e < HV * (W / 4); e += NTHREADS) {
-        int r = e / (W / 4), q = e - r * (W / 4);
-        int gi = i0 - R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
-        st4s(s_atx + o, ld4(in + TXX * P, g, gi, gj));
-        st4s(s_atz + o, ld4(in + TZZ * P, g, gi, gj));
-        st4s(s_atxz + o, ld4(in + TXZ * P, g, gi, gj));
-    }
+    cp_wait_all();
     __syncthreads();
 
     // adjoint stresses on the tile plus an R-cell ring (Adj_update_tau); the
@@ -605,10 +821,7 @@ __global__ void __launch_bounds__(NTHREADS) adj_step(const __grid_constant__ Adj
             avx = avx + (-dt) * ((2.f * dx + dz) * avx + sx);
             avz = avz + (-dt) * ((dx + 2.f * dz) * avz + sz);
         }
-        out[VX * P + co] = avx;
-        out[VZ * P + co] = avz;
-
-        if (gi < glo || gi > g.tnz - R - a.npml || gj < glo || gj > g.tnx - R - a.npml) continue;
+        if (!(gi < glo || gi > g.tnz - R - a.npml || gj < glo || gj > g.tnx - R - a.npml)) {
         const long long sz_ = g.pitch;
         // the new adjoint stresses this CTA wrote above (plain loads: written in this kernel)
         const float atx = out[TXX * P + co], atz = out[TZZ * P + co], atxz = out[TXZ * P + co];
@@ -680,6 +893,12 @@ __global__ void __launch_bounds__(NTHREADS) adj_step(const __grid_constant__ Adj
             G[5 * P + co] += dt2 * (vx * vx * (dxm_tx * dxm_tx + dzm_txz * dzm_txz) +
                                     vz * vz * (dzp_tz * dzp_tz + dxp_txz * dxp_txz));
         }
+        }
+        // the residual the next step injects (Adj_injSrc, elastic_surface.cl:48-71),
+        // added to this step's output after the imaging has read it
+        if (a.epi_row >= 0) inject_epilogue(a, slot, gi, gj, co, avx, avz, out);
+        out[VX * P + co] = avx;
+        out[VZ * P + co] = avz;
     }
 }
 
@@ -1027,6 +1246,53 @@ __global__ void l2_kernel(const float *est, const float *obs, float *res, long l
     }
     for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0) atomicAdd(misfit, 0.5 * acc);
+}
+
+// L2 misfit of one shot group's columns of the traces (CostFunction.l2,
+// fwi_tools.py:1402-1422, on the section of acquisition.py:313-333) and the
+// adjoint sources of those columns.  mean_stress: the two stress keys both
+// hold (txx + tzz) / 2; their residuals are the reference's adjoint sources
+// for txx and tzz (prepare_residual, processing.py:142-158), and for the
+// exact adjoint each stress field gets half their sum (the derivative of the
+// misfit through the mean).
+struct MisfitArgs {
+    const float *traces;   // [5][nt][ncol]
+    const float *obs[5];   // nullable per field: not in the misfit
+    float *res[5];
+    long long nt, ncol, col0, ncols, plane;
+    int mean_stress, exact;
+    double *misfit;
+};
+
+__global__ void misfit_kernel(const MisfitArgs m)
+{
+    double acc = 0.0;
+    const long long n = m.nt * m.ncols;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const long long t = e / m.ncols, o = t * m.ncol + m.col0 + (e - t * m.ncols);
+        if (m.mean_stress) {
+            const float mean = __fdiv_rn(__fadd_rn(m.traces[TXX * m.plane + o], m.traces[TZZ * m.plane + o]), 2.f);
+            const float r1 = m.obs[TXX] ? __fsub_rn(mean, m.obs[TXX][o]) : 0.f;
+            const float r2 = m.obs[TZZ] ? __fsub_rn(mean, m.obs[TZZ][o]) : 0.f;
+            acc += (double)r1 * r1 + (double)r2 * r2;
+            if (m.exact) {
+                const float h = 0.5f * (r1 + r2);
+                m.res[TXX][o] = h;
+                m.res[TZZ][o] = h;
+            } else {
+                if (m.obs[TXX]) m.res[TXX][o] = r1;
+                if (m.obs[TZZ]) m.res[TZZ][o] = r2;
+            }
+        }
+        for (int f = 0; f < 5; ++f) {
+            if (!m.obs[f] || (m.mean_stress && (f == TXX || f == TZZ))) continue;
+            const float r = __fsub_rn(m.traces[f * m.plane + o], m.obs[f][o]);
+            m.res[f][o] = r;
+            acc += (double)r * r;
+        }
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(m.misfit, 0.5 * acc);
 }
 
 __global__ void mean2_kernel(const float *a, const float *b, float *out, long long n)

@@ -526,16 +526,27 @@ AdjArgs base_adj(pyfwi_plan *p, void *ws, const float *const *res)
 }
 
 // backward iteration t of the reference loop (wave_propagation.py:814-848)
+// Residual row injected before backward step t (wave_propagation.py:814-824):
+// t_src starts at nt_ext and steps down at every injection step, the row is
+// t_src - 1 read with numpy's negative-index wrap; -1 if t injects nothing.
+int inj_row_of(const pyfwi_plan *p, int t)
+{
+    const int d = p->geom.dt_scale;
+    if (t < 0 || t % d) return -1;
+    int row = p->geom.nt_ext - 1 - ((p->geom.nt - 1) / d - t / d);
+    if (row < 0) row += p->geom.nt_ext;
+    return row;
+}
+
 int adjoint_iter(pyfwi_plan *p, void *ws, AdjArgs &a, int t, int &t_src, int &ping, float *adj, int n, cudaStream_t st)
 {
-    if (t % p->geom.dt_scale == 0) {
-        int row = t_src - 1;
-        if (row < 0) row += p->geom.nt_ext;  // numpy negative index
-        a.inj_row = row;
-        t_src -= 1;
-    } else {
-        a.inj_row = -1;
-    }
+    if (t % p->geom.dt_scale == 0) t_src -= 1;
+    // the tile kernel adds the residual of the next step (t - 1; step 0 never
+    // runs) to its own output, so only the first backward step injects into
+    // its input with a separate launch
+    const bool epilogue = p->ast_w == 0;
+    a.inj_row = (!epilogue || t == p->geom.nt - 1) ? inj_row_of(p, t) : -1;
+    a.epi_row = epilogue && t - 1 >= 1 ? inj_row_of(p, t - 1) : -1;
     a.in = adj + (long long)ping * p->state;
     a.out = adj + (long long)(1 - ping) * p->state;
     a.in_stride = a.out_stride = 2 * p->state;
@@ -638,34 +649,75 @@ int exact_backward(pyfwi_plan *p, void *ws, const float *const *residual, int s0
 }
 
 // Everything pyfwi_gradient enqueues (host state is updated by the caller).
+// The fused misfit evaluation (pyfwi_misfit_gradient): per shot group,
+// forward with traces, then the L2 residual of the group's traces, then the
+// group's adjoint, so a layout of several groups models each group once.
+struct Misfit {
+    float *traces;        // [5][nt_ext][ns*nr] modelled traces (written)
+    const float *obs[5];  // observed traces per field (nullable)
+    float *res[5];        // adjoint sources (written where used)
+    int mean_stress;      // the stress keys hold (txx + tzz) / 2
+    double *misfit;
+};
+
+int misfit_group(pyfwi_plan *p, const Misfit &mf, int s0, int n, cudaStream_t st)
+{
+    const pyfwi_geometry &G = p->geom;
+    MisfitArgs m;
+    m.traces = mf.traces;
+    for (int c = 0; c < 5; ++c) {
+        m.obs[c] = mf.obs[c];
+        m.res[c] = mf.res[c];
+    }
+    m.nt = G.nt_ext;
+    m.ncol = (long long)G.ns * G.nr;
+    m.col0 = (long long)s0 * G.nr;
+    m.ncols = (long long)n * G.nr;
+    m.plane = (long long)G.nt_ext * G.ns * G.nr;
+    m.mean_stress = mf.mean_stress;
+    m.exact = p->exact_adj;
+    m.misfit = mf.misfit;
+    misfit_kernel<<<grid_blocks(m.nt * m.ncols), 256, 0, st>>>(m);
+    p->launches++;
+    CKL();
+    return PYFWI_OK;
+}
+
 int gradient_enqueue(pyfwi_plan *p, void *ws, const float *const *residual, int32_t param, float *grad, float *raw,
-                     cudaStream_t st)
+                     cudaStream_t st, const Misfit *mf = nullptr)
 {
     int rc;
     const pyfwi_geometry &G = p->geom;
     float *gacc = at<float>(ws, p->o_gacc);
     float *adj = at<float>(ws, p->o_adj);
     CK(cudaMemsetAsync(gacc, 0, (size_t)p->nacc * p->g.plane * p->G * sizeof(float), st));
+    if (mf) {
+        residual = mf->res;
+        CK(cudaMemsetAsync(mf->traces, 0, 5 * (size_t)G.nt_ext * G.ns * G.nr * sizeof(float), st));
+        CK(cudaMemsetAsync(mf->misfit, 0, sizeof(double), st));
+    }
     AdjArgs a = base_adj(p, ws, residual);
 
     for (int grp = 0; grp < p->ngroups; ++grp) {
         int s0 = grp * p->G, n = std::min(p->G, G.ns - s0);
         a.shot0 = s0;
+        if (mf) {  // model this group, then its residual
+            rc = p->opt.checkpoint == PYFWI_CKPT_EXACT ? exact_pass(p, ws, s0, n, mf->traces, st)
+                                                         : reverse_pass(p, ws, s0, n, mf->traces, st);
+            if (rc) return rc;
+            rc = misfit_group(p, *mf, s0, n, st);
+            if (rc) return rc;
+        } else if (p->opt.checkpoint == PYFWI_CKPT_EXACT && (p->ngroups > 1 || !p->fwd_valid)) {
+            rc = exact_pass(p, ws, s0, n, nullptr, st);  // the states of this group are gone
+            if (rc) return rc;
+        }
         for (int q = 0; q < n; ++q) CK(cudaMemsetAsync(adj + 2 * q * p->state, 0, p->state * sizeof(float), st));
         int ping = 0, t_src = G.nt_ext;
         if (p->exact_adj) {
-            if (p->ngroups > 1 || !p->fwd_valid) {
-                rc = exact_pass(p, ws, s0, n, nullptr, st);
-                if (rc) return rc;
-            }
             const float *zero[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
             rc = exact_backward(p, ws, residual ? residual : zero, s0, n, st);
             if (rc) return rc;
         } else if (p->opt.checkpoint == PYFWI_CKPT_EXACT) {
-            if (p->ngroups > 1 || !p->fwd_valid) {
-                rc = exact_pass(p, ws, s0, n, nullptr, st);
-                if (rc) return rc;
-            }
             StepArgs f = base_step(p, ws);
             f.shot0 = s0;
             for (int m = p->M - 1; m >= 0; --m) {
@@ -1142,6 +1194,40 @@ int pyfwi_gradient(pyfwi_plan *p, void *ws, size_t bytes, const float *const *re
     if (rc) return rc;
     if (p->opt.checkpoint == PYFWI_CKPT_EXACT && p->M > 1) p->fwd_valid = false;  // last segment overwritten
     if (p->opt.checkpoint == PYFWI_CKPT_EXACT && p->ngroups > 1) p->fwd_valid = true;  // passes were redone anyway
+    return PYFWI_OK;
+}
+
+int pyfwi_misfit_gradient(pyfwi_plan *p, void *ws, size_t bytes, const float *src_vals, int32_t n_src,
+                          const float *const *observed, int32_t mean_stress, float *const *adjoint_source,
+                          int32_t param, float *traces, float *grad, double *misfit, void *stream)
+{
+    if (!p || !observed || !adjoint_source || !traces || !grad || !misfit || (n_src > 0 && !src_vals) || n_src < 0 ||
+        (param != PYFWI_PARAM_LMD && param != PYFWI_PARAM_DV))
+        return fail(PYFWI_E_INVALID, "bad argument");
+    int rc = check_ws(p, ws, bytes);
+    if (rc) return rc;
+    if (!p->model_set) return fail(PYFWI_E_STATE, "pyfwi_set_model must come first");
+    Misfit mf;
+    mf.traces = traces;
+    mf.mean_stress = mean_stress != 0;
+    mf.misfit = misfit;
+    bool any = false;
+    for (int c = 0; c < 5; ++c) {
+        mf.obs[c] = observed[c];
+        mf.res[c] = adjoint_source[c];
+        if (observed[c] && !adjoint_source[c]) return fail(PYFWI_E_INVALID, "field %d observed but no adjoint buffer", c);
+        any = any || observed[c];
+    }
+    if (!any) return fail(PYFWI_E_INVALID, "no observed field");
+    if (mf.mean_stress && ((observed[TXX] && !adjoint_source[TZZ]) || (observed[TZZ] && !adjoint_source[TXX])))
+        return fail(PYFWI_E_INVALID, "mean_stress needs adjoint buffers for both stress fields");
+    p->src_vals.assign(src_vals, src_vals + 4 * (size_t)n_src);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    rc = gradient_enqueue(p, ws, nullptr, param, grad, nullptr, st, &mf);
+    if (rc) return rc;
+    // the last group's states are in the store: a pyfwi_gradient may follow
+    // without another forward only if there is one group and nothing was recomputed
+    p->fwd_valid = p->ngroups == 1 && (p->opt.checkpoint != PYFWI_CKPT_EXACT || p->M == 1);
     return PYFWI_OK;
 }
 

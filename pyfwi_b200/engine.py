@@ -85,6 +85,23 @@ class Plan:
         N.check(self.lib.pyfwi_launch_count(self.handle, ctypes.byref(c)))
         return c.value
 
+    def misfit_gradient(self, src_vals, observed, mean_stress, adjoint, param, traces=None):
+        """pyfwi_misfit_gradient: observed / adjoint are lists of 5 device
+        tensors [nt_ext, ns*nr] or None.  Returns (grad [3, nz, nx], misfit
+        0-d float64 tensor, traces [5, nt_ext, ns*nr])."""
+        sv = np.ascontiguousarray(src_vals, np.float32).reshape(-1, 4)
+        if traces is None:
+            traces = torch.empty((5, self.nt_ext, self.ns * self.nr), dtype=torch.float32, device=self.device)
+        grad = torch.empty((3, self.nz, self.nx), dtype=torch.float32, device=self.device)
+        misfit = torch.zeros((), dtype=torch.float64, device=self.device)
+        N.check(self.lib.pyfwi_misfit_gradient(self.handle, self.ws, self.ws_bytes,
+                                               sv.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(sv.shape[0]),
+                                               _ptr_array(observed), int(bool(mean_stress)), _ptr_array(adjoint),
+                                               int(param), _ptr(traces), _ptr(grad), _ptr(misfit),
+                                               _stream(self.device)))
+        self._keep = (observed, adjoint)
+        return grad, misfit, traces
+
     def check_device(self):
         """Synchronise the device stream and raise NativeError if a streaming
         kernel gave up waiting for a row copy since the last check."""
@@ -154,6 +171,10 @@ class Plan:
                                         _stream(self.device)))
         self._res_keep = res
         return grad.clone() if self.opts.graph else grad
+
+
+def _ptr_array(ts):
+    return (ctypes.c_void_p * 5)(*[(t.data_ptr() if t is not None else None) for t in ts])
 
 
 def mean2(a, b):

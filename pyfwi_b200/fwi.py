@@ -12,6 +12,7 @@ import numpy as np
 import torch
 from scipy.optimize import fmin_cg, fmin_l_bfgs_b
 
+from . import acquisition as acq
 from . import fwi_tools as tools
 from .processing import COMPONENTS, prepare_residual
 from .wave_propagation import WavePropagator
@@ -122,7 +123,12 @@ class FWI(WavePropagator):
             raise NotImplementedError("band-limited misfit (freq) is not provided")
         m_old = self.vec2dict(np.copy(m0), self.nz, self.nx)
         m_new = self.model_to_dv(m_old, self.param_functions_args)
-        d_est = self.forward_modeling({k: self._to_device(m_new[k]) for k in ("vp", "vs", "rho")}, show=False)
+        model = {k: self._to_device(m_new[k]) for k in ("vp", "vs", "rho")}
+        if self.sd == 1 and set(self.d_obs) == set(acq.section_keys(self.components)):
+            # forward, misfit and gradient fused per shot group (same result)
+            rms, grad_dv = self.misfit_gradient(model, self.d_obs, parameterization="dv")
+            return self._finish(float(rms.item()), grad_dv, m_old)
+        d_est = self.forward_modeling(model, show=False)
         d_est = {k: self.sd * v for k, v in d_est.items()}
         rms = torch.zeros((), dtype=torch.float64, device=self.device)
         adj = {}
@@ -134,12 +140,16 @@ class FWI(WavePropagator):
                 rms += r
                 adj[k] = res[k]
         grad_dv = self.gradient(adj, parameterization="dv")
+        return self._finish(float(rms.item()), grad_dv, m_old)
+
+    def _finish(self, rms, grad_dv, m_old):
+        """Gradient vector from the (vp, vs, rho) device gradient (fwi.py:243-252)."""
         grad_dv = {k: v.cpu().numpy() for k, v in grad_dv.items()}
         grad = self.grad_from_dv(grad_dv, self.param_functions_args, m_old)
         params = [*grad]
         for q in range(3):
             grad[params[q]] = grad[params[q]] * self.grad_coeff[q]
-        return float(rms.item()), self.dict2vec(grad)
+        return rms, self.dict2vec(grad)
 
     def fprime_single(self, m0, m_1, m1, freq):
         mtotal = np.float32(np.hstack((m_1, m0, m1)))

@@ -305,24 +305,66 @@ class WavePreparation:
         self.segment, self.shot_batch = seg, batch
         self._tile, self._adj_tile = variants[0], (variants[1] - 1 if variants[1] else variants[0])
 
+    # Layout cost model, in units of one forward step of one cell of one shot:
+    # an adjoint+imaging step costs about 1.9 of them; a forward step has a
+    # fixed cost of about 4.6e5 and an adjoint step about 2.3e6 (B200, fitted
+    # to 3 and 64 shots on 593,600 cells: forward 6 us + 7.7 us per shot,
+    # adjoint 30 us + 14.4 us per shot).
+    COST_ADJ, COST_FWD_STEP, COST_ADJ_STEP = 1.9, 4.6e5, 2.3e6
+
     def _auto_layout(self, geom, opts, seg, batch):
-        """Largest segment (fewest recomputed steps) and shot batch whose
-        workspace fits in free device memory."""
+        """Shot batch and recompute segment of the exact checkpoint mode.
+
+        Among the layouts whose workspace fits in free device memory, the one
+        with the least modelled time for a misfit_gradient call: per group of
+        b shots, nt forward steps plus (M - 1) * segment recomputed forward
+        steps (M = ceil(nt / segment)) and nt adjoint steps, each step costing
+        its cells x shots plus a fixed cost per step.  Storing every step of a
+        few shots beats recomputing a large batch only where the grid is large
+        enough to fill the GPU with a few shots."""
         free, _ = torch.cuda.mem_get_info(self.device)
         traces = 5 * self.nt_ext * int(self.ns) * int(self.nr) * 4
         budget = int(0.9 * free) - 4 * traces - (256 << 20)
         nt, ns = int(self.nt), int(self.ns)
-        batches = [batch] if batch else sorted({ns, (ns + 1) // 2, (ns + 3) // 4, 1}, reverse=True)
-        for b in batches:
-            k = 1
-            while True:
-                s = seg or -(-nt // k)
-                if Plan.workspace_bytes(geom, opts(s, b), ns) <= budget:
-                    return s, b
-                if seg or s * s < nt:
-                    break
-                k += 1
-        raise MemoryError("the survey does not fit in device memory (%.1f GB free)" % (free / 2 ** 30))
+        cells = float(int(self.tnz) * int(self.tnx))
+        memo = {}
+
+        def fits(s, b):
+            if (s, b) not in memo:
+                memo[s, b] = Plan.workspace_bytes(geom, opts(s, b), ns) <= budget
+            return memo[s, b]
+
+        def largest_segment(b):
+            if seg:
+                return seg if fits(seg, b) else None
+            if fits(nt, b):
+                return nt
+            # the store holds ceil(nt / s) + s states: growing for s >= sqrt(nt)
+            lo = int(np.ceil(np.sqrt(nt)))
+            if not fits(lo, b):
+                return None
+            hi = nt
+            while hi - lo > 1:
+                mid = (lo + hi) // 2
+                lo, hi = (mid, hi) if fits(mid, b) else (lo, mid)
+            return lo
+
+        def group_cost(s, b):
+            m = -(-nt // s)
+            fwd = nt + (m - 1) * s
+            return fwd * (b * cells + self.COST_FWD_STEP) + nt * (b * cells * self.COST_ADJ + self.COST_ADJ_STEP)
+
+        best = None
+        for b in ([batch] if batch else range(ns, 0, -1)):
+            s = largest_segment(b)
+            if s is None:
+                continue
+            cost = (ns // b) * group_cost(s, b) + (group_cost(s, ns % b) if ns % b else 0.0)
+            if best is None or cost < best[0]:
+                best = (cost, s, b)
+        if best is None:
+            raise MemoryError("the survey does not fit in device memory (%.1f GB free)" % (free / 2 ** 30))
+        return best[1], best[2]
 
     # ---- helpers ---------------------------------------------------------
     def _to_device(self, x):
@@ -429,6 +471,49 @@ class WavePropagator(WavePreparation):
         if as_numpy:
             out = {k: v.cpu().numpy() for k, v in out.items()}
         return out
+
+    def misfit_gradient(self, model0, d_obs, parameterization="dv"):
+        """The misfit and gradient that FWI.fprime evaluates (fwi.py:229-252:
+        forward_modeling, CostFunction('l2') on the section, gradient), in
+        one library call that runs each shot group's forward pass, residual
+        and adjoint in turn (pyfwi_misfit_gradient), so a layout of several
+        shot groups models every group once.  d_obs: the observed section
+        (the dict forward_modeling returns, '2d' or '3d', numpy or torch).
+        Returns (rms, gradient dict); rms is a float for numpy input, else a
+        0-d float64 device tensor."""
+        if self.acq_type == 2 and self.n_well_rec:  # the section reorders traces: separate calls
+            d_est = self.forward_modeling(model0)
+            rms, res = tools.CostFunction("l2")(d_est, d_obs)
+            return rms, self.gradient(res, parameterization=parameterization)
+        as_numpy = not isinstance(model0["vp"], torch.Tensor)
+        vp, vs, rho = (self._to_device(model0[k]) for k in ("vp", "vs", "rho"))
+        damp_x = torch.from_numpy(np.ascontiguousarray(self.dx_pml[0, :]))
+        damp_z = torch.from_numpy(np.ascontiguousarray(self.dz_pml[:, 0]))
+        self.plan.set_model(vp, vs, rho, damp_x, damp_z)
+        self._model_dev = (vp, vs, rho)
+        nt, nrs = int(self.nt_ext), int(self.nr) * int(self.ns)
+        obs = [None] * 5
+        for k, v in d_obs.items():
+            f = FIELDS.index(k)
+            if v.ndim == 3:  # (nt, nr, ns) -> (nt, ns*nr)
+                v = (np.transpose(v, (0, 2, 1)) if isinstance(v, np.ndarray) else v.permute(0, 2, 1))
+            obs[f] = self._to_device(v).reshape(nt, nrs).contiguous()
+        mean_stress = self.components == 0
+        adj = [None] * 5
+        for f in range(5):
+            if obs[f] is not None or (mean_stress and f in (2, 3) and (obs[2] is not None or obs[3] is not None)):
+                adj[f] = torch.empty((nt, nrs), dtype=torch.float32, device=self.device)
+        param = N.PARAM_DV if parameterization == "dv" else N.PARAM_LMD
+        g, rms, self._traces = self.plan.misfit_gradient(self._wavelet, obs, mean_stress, adj, param, self._traces)
+        self._adjoint_source = {FIELDS[f]: adj[f] for f in range(5) if adj[f] is not None}
+        if float(self.g_smooth) > 1e-15:
+            g = smooth(g, self.g_smooth)
+        names = ("vp", "vs", "rho") if parameterization == "dv" else ("lam", "mu", "rho")
+        out = {n: g[q] for q, n in enumerate(names)}
+        self._check_device(as_numpy)
+        if as_numpy:
+            return float(rms.item()), {k: v.cpu().numpy() for k, v in out.items()}
+        return rms, out
 
     def _trace_adjoint(self, planes):
         """Exact adjoint: the section's dJ/d(section) per key -> dJ/d(raw

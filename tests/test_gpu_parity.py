@@ -166,3 +166,33 @@ def test_tensor_inputs_stay_on_device():
     d2 = W2.forward_modeling(case["model_est"])
     for k in d:
         assert np.array_equal(d[k].cpu().numpy(), d2[k])
+
+
+@pytest.mark.parametrize("name,extra", [("c1", {}), ("tiny_dtscale", {"segment": 0, "shot_batch": 1}),
+                                        ("tiny_chpr", {}), ("tiny_s8", {"segment": 9, "shot_batch": 3}),
+                                        ("tiny_s8", {"adjoint": "exact", "shot_batch": 2, "segment": 0})])
+def test_misfit_gradient_matches_separate_calls(name, extra):
+    """misfit_gradient (forward, residual and adjoint fused per shot group)
+    gives the misfit and gradient of forward_modeling + CostFunction('l2') +
+    gradient, also when the shots run in several groups."""
+    import torch
+    from pyfwi_b200 import fwi_tools
+    case = cases.by_name(name)
+    g = load_golden(name)
+    obs = _golden_section(g, "d_obs_")
+    W = product(case, **extra)
+    d_est = W.forward_modeling(case["model_est"])
+    rms_a, res = fwi_tools.CostFunction("l2")(d_est, obs)
+    grad_a = W.gradient(res, parameterization=case["param"])
+    W2 = product(case, **extra)
+    rms_b, grad_b = W2.misfit_gradient(case["model_est"], obs, parameterization=case["param"])
+    torch.cuda.synchronize()
+    assert abs(rms_b - rms_a) <= 1e-6 * abs(rms_a), (rms_a, rms_b)
+    for k in grad_a:
+        assert rel_l2(grad_b[k], grad_a[k]) <= 1e-6, k
+    if "adjoint" not in extra:
+        for k in grad_b:
+            assert rel_l2(grad_b[k], g["grad_" + k]) < GRAD_TOL, k
+    # the modelled traces are those of forward_modeling
+    for k, v in W2.seismogram.items():
+        assert np.array_equal(v, W.seismogram[k]), k
