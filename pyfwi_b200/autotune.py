@@ -9,7 +9,8 @@ hand and picks the fastest forward and the fastest adjoint variant
 independently (``pyfwi_options.tile`` and ``adj_tile``).
 
 Timing uses the library's own per-step CUDA events (``pyfwi_profile_*``) on a
-plan of ``steps`` time steps and up to ``max_shots`` shots per launch.
+plan of ``steps`` time steps and as many shots per launch as the survey's
+plan will run (up to ``max_shots``).
 Results are kept per process, keyed by device, half order, padded grid,
 shots per launch and energy accumulation; set ``PYFWI_B200_TUNE_CACHE`` to a
 JSON file path to keep them across processes.
@@ -85,12 +86,17 @@ def time_variant(geom, srcx, srcz, energy, shots, variant, device, steps=16):
     return out
 
 
-def tune(geom, srcx, srcz, energy, shots_per_launch, device, steps=16, max_shots=8, variants=None):
+def tune(geom, srcx, srcz, energy, shots_per_launch, device, steps=16, max_shots=64, variants=None):
     """(forward variant, adjoint variant, table) for plans of `geom` running
     `shots_per_launch` shots per launch.  table: {variant: (fwd ms, adj ms)}
-    per launch of min(shots_per_launch, max_shots) shots."""
+    per launch of min(shots_per_launch, max_shots) shots (fewer if the short
+    plans would not fit in a quarter of the free device memory)."""
     device = torch.device(device)
-    shots = int(max(1, min(shots_per_launch, max_shots, len(srcx))))
+    tnz, tnx = geom.nz + 2 * geom.npml, geom.nx + 2 * geom.npml
+    state = 5 * 4 * (tnz + 16) * (-(-(tnx + 16) // 32) * 32)
+    free, _ = torch.cuda.mem_get_info(device)
+    fit = max(1, int(0.25 * free) // ((steps + 6) * state))
+    shots = int(max(1, min(shots_per_launch, max_shots, len(srcx), fit)))
     key = _key(device, geom, shots, energy)
     if key in _CACHE:
         return _CACHE[key]

@@ -110,6 +110,11 @@ struct pyfwi_plan {
     } tmaps[2];
 };
 
+// The static-scratch entry point clears its array before every call: the
+// plan must then initialise that workspace again (zero frames, source cells)
+// in pyfwi_set_model.  Hidden from the library's exported symbols.
+__attribute__((visibility("hidden"))) void pyfwi_plan_workspace_cleared(pyfwi_plan *p) { p->ws_initialised = nullptr; }
+
 // Trace dimensions of a plan for the static-scratch entry point; hidden from
 // the library's exported symbols.
 __attribute__((visibility("hidden"))) void pyfwi_plan_trace_dims(const pyfwi_plan *p, int *nt_ext, int *ns, int *nr)
@@ -1122,13 +1127,16 @@ int pyfwi_set_model(pyfwi_plan *p, void *ws, size_t bytes, const float *vp, cons
     if (rc) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (p->ws_initialised != ws) {
-        // frames and padding of every plane must read as zero
+        // frames and padding of every plane must read as zero; the source
+        // cells are constant for the plan (later calls copy nothing from the
+        // host, so they may be captured in a CUDA graph)
         CK(cudaMemsetAsync(ws, 0, p->total, st));
+        CK(cudaMemcpyAsync(at<int>(ws, p->o_src), p->srcx.data(), p->geom.ns * sizeof(int), cudaMemcpyHostToDevice,
+                           st));
+        CK(cudaMemcpyAsync(at<int>(ws, p->o_src) + p->geom.ns, p->srcz.data(), p->geom.ns * sizeof(int),
+                           cudaMemcpyHostToDevice, st));
         p->ws_initialised = ws;
     }
-    CK(cudaMemcpyAsync(at<int>(ws, p->o_src), p->srcx.data(), p->geom.ns * sizeof(int), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(at<int>(ws, p->o_src) + p->geom.ns, p->srcz.data(), p->geom.ns * sizeof(int),
-                       cudaMemcpyHostToDevice, st));
     int *vmax = at<int>(ws, p->o_hdr);
     CK(cudaMemsetAsync(vmax, 0, sizeof(int), st));
     long long nm = (long long)p->geom.nz * p->geom.nx;

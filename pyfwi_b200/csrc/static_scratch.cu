@@ -28,10 +28,11 @@
 #include <mutex>
 #include <string>
 
-// Defined in pyfwi_b200.cu: the message pyfwi_last_error() returns, and the
-// trace dimensions of a plan.
+// Defined in pyfwi_b200.cu: the message pyfwi_last_error() returns, the
+// trace dimensions of a plan, and the notice that its workspace was cleared.
 void pyfwi_set_error(const char *msg);
 void pyfwi_plan_trace_dims(const pyfwi_plan *p, int *nt_ext, int *ns, int *nr);
+void pyfwi_plan_workspace_cleared(pyfwi_plan *p);
 
 namespace {
 
@@ -114,6 +115,7 @@ extern "C" int pyfwi_gradient_static(pyfwi_plan *plan, const float *vp, const fl
         pyfwi_set_error((std::string("cudaMemsetAsync: ") + cudaGetErrorString(e)).c_str());
         return PYFWI_E_CUDA;
     }
+    pyfwi_plan_workspace_cleared(plan);
     char *b = static_cast<char *>(base);
     float *traces = reinterpret_cast<float *>(b + o_traces);
     if ((rc = pyfwi_set_model(plan, base, ws_bytes, vp, vs, rho, damp_x, damp_z, stream))) return rc;

@@ -393,9 +393,7 @@ class WavePropagator(WavePreparation):
             warnings.warn("show=True: live wavefield plotting is not available; ignored")
         as_numpy = not isinstance(model0["vp"], torch.Tensor)
         vp, vs, rho = (self._to_device(model0[k]) for k in ("vp", "vs", "rho"))
-        damp_x = torch.from_numpy(np.ascontiguousarray(self.dx_pml[0, :]))
-        damp_z = torch.from_numpy(np.ascontiguousarray(self.dz_pml[:, 0]))
-        self.plan.set_model(vp, vs, rho, damp_x, damp_z)
+        self.plan.set_model(vp, vs, rho, *self._damping())
         self._traces = self.plan.forward(self._wavelet, self._traces)
         self._model_dev = (vp, vs, rho)
         data = self._section(self._traces)
@@ -404,11 +402,22 @@ class WavePropagator(WavePreparation):
             data = {k: v.cpu().numpy() for k, v in data.items()}
         return data
 
+    def _damping(self):
+        """The damping profiles per column and per row (the reference's 2-D
+        dx_pml / dz_pml are separable), on the device, uploaded once."""
+        if getattr(self, "_damp_dev", None) is None:
+            self._damp_dev = tuple(torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(self.device)
+                                   for a in (self.dx_pml[0, :], self.dz_pml[:, 0]))
+        return self._damp_dev
+
     def _check_device(self, synchronous):
         """Raise if a streaming kernel stopped early.  Reading the error word
         synchronises, so it is done where the call synchronises anyway (host
-        results) or where a streaming kernel ran."""
-        if synchronous or self.plan.opts.tile >= 3:
+        results) or where a streaming kernel ran, never inside a CUDA-graph
+        capture."""
+        if torch.cuda.is_current_stream_capturing():
+            return
+        if synchronous or self.plan.opts.tile >= 3 or self.plan.opts.adj_tile >= 4:
             self.plan.check_device()
 
     def _section(self, traces):
@@ -487,9 +496,7 @@ class WavePropagator(WavePreparation):
             return rms, self.gradient(res, parameterization=parameterization)
         as_numpy = not isinstance(model0["vp"], torch.Tensor)
         vp, vs, rho = (self._to_device(model0[k]) for k in ("vp", "vs", "rho"))
-        damp_x = torch.from_numpy(np.ascontiguousarray(self.dx_pml[0, :]))
-        damp_z = torch.from_numpy(np.ascontiguousarray(self.dz_pml[:, 0]))
-        self.plan.set_model(vp, vs, rho, damp_x, damp_z)
+        self.plan.set_model(vp, vs, rho, *self._damping())
         self._model_dev = (vp, vs, rho)
         nt, nrs = int(self.nt_ext), int(self.nr) * int(self.ns)
         obs = [None] * 5

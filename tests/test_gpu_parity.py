@@ -85,20 +85,25 @@ def test_exact_checkpoint_segments_are_bit_identical():
 
 
 def test_tile_variants_agree():
-    """Tile kernels of every height give identical bits; streaming kernels
-    (other FMA grouping) agree to float32 rounding."""
+    """Tile kernels of every height give identical bits (forward and
+    gradient); streaming kernels (other FMA grouping) agree to float32
+    rounding."""
     case = cases.tiny_dxr()
+    g = load_golden("tiny_dxr")
+    res = l2_residual_np(_golden_section(g, "d_est_"), _golden_section(g, "d_obs_"))
     base = None
     for tile in range(6):
         W = product(case, tile=tile)
         d = W.forward_modeling(case["model_est"])
+        gr = W.gradient(res, parameterization=case["param"])
         if base is None:
-            base = d
-        for k in d:
-            if tile < 3:
-                assert np.array_equal(d[k], base[k]), (tile, k)
-            else:
-                assert rel_l2(d[k], base[k]) < 1e-6, (tile, k)
+            base = (d, gr)
+        for out, ref in ((d, base[0]), (gr, base[1])):
+            for k in out:
+                if tile < 3:
+                    assert np.array_equal(out[k], ref[k]), (tile, k)
+                else:
+                    assert rel_l2(out[k], ref[k]) < 1e-6, (tile, k)
 
 
 @pytest.mark.parametrize("chunk", [3, 8, 1000])
