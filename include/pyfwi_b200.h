@@ -190,6 +190,16 @@ int pyfwi_misfit_gradient(pyfwi_plan *plan, void *workspace, size_t bytes, const
                           const float *const *observed, int32_t mean_stress, float *const *adjoint_source,
                           int32_t parameterization, float *traces, float *grad, double *misfit, void *stream);
 
+/* Low-pass filter of the multiscale misfit (lowpass / adj_lowpass,
+ * fwi_tools.py:1188-1258): each of n_planes device planes [nt][ncols] of
+ * traces (time along rows) is multiplied along time by `response`, the
+ * device nt x nt matrix of the filter (symmetric; built on the host from the
+ * Butterworth design, pyfwi_b200.fwi_tools.lowpass_response), as an FP32
+ * GEMM.  in and out must not overlap.  Uses one cuBLAS handle per calling
+ * thread and device, created on first use. */
+int pyfwi_lowpass(const float *response, const float *in, float *out, int32_t nt, int64_t ncols, int32_t n_planes,
+                  void *stream);
+
 /* Trace section (acquisition.py:313-333): out = (a + b) / 2 elementwise. */
 int pyfwi_mean2(const float *a, const float *b, float *out, int64_t n, void *stream);
 

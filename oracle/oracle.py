@@ -196,6 +196,22 @@ def grad_lmd_to_vd(glam, gmu, grho, lam, mu, rho):
 FIELDS = ["vx", "vz", "taux", "tauz", "tauxz"]
 
 
+def lowpass(x, highcut, fn, order, axis=1):
+    """lowpass and adj_lowpass of fwi_tools.py:1188-1258 (the two apply the
+    same product), in float64: traces (planes, nt, ncols) padded with 512
+    zeros along time, FFT, times h and conj(h) (freqz of the Butterworth
+    design on the whole circle), real inverse FFT, first nt samples."""
+    from scipy.signal import butter, freqz
+    assert axis == 1
+    x = np.concatenate([np.asarray(x, np.float64), np.zeros((x.shape[0], 512, x.shape[2]))], axis=1)
+    n = x.shape[1]
+    X = np.fft.fft(x, n=n, axis=1)
+    b, a = butter(order, 2 * highcut / fn, btype="lowpass", output="ba")
+    _, h = freqz(b, a, worN=n, whole=True)
+    X = np.conjugate(h)[None, :, None] * (h[None, :, None] * X)
+    return np.fft.ifft(X, n=n, axis=1).real[:, :-512, :]
+
+
 class OracleWavePropagator:
     """CPU oracle with the reference ``WavePropagator`` interface.
 

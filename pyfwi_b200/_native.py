@@ -66,6 +66,7 @@ def lib():
     L.pyfwi_mean2.argtypes = [_P, _P, _P, ctypes.c_int64, _P]
     L.pyfwi_misfit_gradient.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_float), _i32,
                                         ctypes.POINTER(_P), _i32, ctypes.POINTER(_P), _i32, _P, _P, _P, _P]
+    L.pyfwi_lowpass.argtypes = [_P, _P, _P, _i32, ctypes.c_int64, _i32, _P]
     L.pyfwi_smooth.argtypes = [_P, _P, _P, _i32, _i32, _i32, ctypes.POINTER(ctypes.c_double), _i32, _P]
     L.pyfwi_tile_count.argtypes = [_i32]
     L.pyfwi_launch_count.argtypes = [_P, ctypes.POINTER(ctypes.c_int64)]
@@ -81,7 +82,7 @@ def lib():
     for name in ("pyfwi_plan_create", "pyfwi_plan_destroy", "pyfwi_workspace_size", "pyfwi_set_model",
                  "pyfwi_forward", "pyfwi_gradient", "pyfwi_l2_residual", "pyfwi_mean2", "pyfwi_tile_count",
                  "pyfwi_launch_count", "pyfwi_profile_enable", "pyfwi_profile_read", "pyfwi_device_error",
-                 "pyfwi_smooth", "pyfwi_misfit_gradient"):
+                 "pyfwi_smooth", "pyfwi_misfit_gradient", "pyfwi_lowpass"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libpyfwi_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "pyfwi_b200.cu"), os.path.join(HERE, "csrc", "static_scratch.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("pyfwi_b200.cu", "static_scratch.cu", "lowpass.cu")]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + \
     [os.path.join(ROOT, "include", "pyfwi_b200.h")]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -37,7 +37,7 @@ def build(force=False, verbose=False):
     if not force and up_to_date():
         return LIB
     tmp = LIB + ".tmp%d" % os.getpid()
-    cmd = [nvcc()] + NVCC_FLAGS + SOURCES + ["-o", tmp]
+    cmd = [nvcc()] + NVCC_FLAGS + SOURCES + ["-lcublas", "-o", tmp]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)

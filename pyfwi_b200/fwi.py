@@ -5,8 +5,9 @@ Same constructor and ``__call__(m0, method, iter, freqs, n_params, k_0,
 k_end)``; SciPy's conjugate gradient / L-BFGS-B drive ``fprime_single`` as in
 the reference.  Each misfit evaluation runs forward modelling, the L2
 residual and the adjoint gradient on the device; only the model and
-gradient vectors cross to the host for SciPy.  Regularisation terms (TV,
-Tikhonov, prior, parameter relations) and band-limited misfits are not
+gradient vectors cross to the host for SciPy.  The multiscale frequencies
+(`freqs`) low-pass the data on the device (fwi_tools.lowpass).
+Regularisation terms (TV, Tikhonov, prior, parameter relations) are not
 provided: asking for them raises."""
 import numpy as np
 import torch
@@ -118,12 +119,21 @@ class FWI(WavePropagator):
         return mtotal, hist
 
     def fprime(self, m0, freq):
-        """Misfit and its gradient (as a vector) at model vector m0."""
-        if freq:
-            raise NotImplementedError("band-limited misfit (freq) is not provided")
+        """Misfit and its gradient (as a vector) at model vector m0; with
+        `freq` both data are low-passed first (cost_seismic, fwi.py:238-240)."""
         m_old = self.vec2dict(np.copy(m0), self.nz, self.nx)
         m_new = self.model_to_dv(m_old, self.param_functions_args)
         model = {k: self._to_device(m_new[k]) for k in ("vp", "vs", "rho")}
+        if freq:
+            d_est = self.forward_modeling(model, show=False)
+            d_est = {k: self.sd * v for k, v in d_est.items()}
+            keys = [k for k in COMPONENTS if k in d_est or k in self.d_obs]
+            like = next(iter(d_est.values()))
+            est = {k: d_est[k] if k in d_est else torch.zeros_like(like) for k in keys}
+            obs = {k: self.d_obs[k] if k in self.d_obs else torch.zeros_like(like) for k in keys}
+            rms, adj = tools.cost_seismic(est, obs, fun=tools.CostFunction("l2"), fn=self.fn, freq=freq, order=3,
+                                          axis=1)
+            return self._finish(float(rms.item()), self.gradient(adj, parameterization="dv"), m_old)
         if self.sd == 1 and set(self.d_obs) == set(acq.section_keys(self.components)):
             # forward, misfit and gradient fused per shot group (same result)
             rms, grad_dv = self.misfit_gradient(model, self.d_obs, parameterization="dv")

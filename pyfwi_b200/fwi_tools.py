@@ -106,15 +106,100 @@ class CostFunction:
         return l2_residual(dest, dobs)
 
 
+LOWPASS_PADDING = 512  # zeros the reference appends to every trace before its FFT
+_RESPONSES = {}
+
+
+def lowpass_response(nt, highcut, fn, order=1):
+    """The reference's zero-phase low-pass (lowpass / adj_lowpass,
+    fwi_tools.py:1188-1258) as an nt x nt float32 matrix K, with
+    lowpass(x)[t] = sum_s K[t][s] x[s] along time.
+
+    The reference filters in the frequency domain: traces padded to
+    n = nt + 512 samples, multiplied by h and conj(h) (h: freqz of
+    butter(order, 2 highcut / fn) on the whole circle) and cut back to nt
+    samples of the real inverse FFT.  That is a circular convolution with
+    g = real(ifft(conj(h) h)), so K[t][s] = g[(t - s) mod n]; adj_lowpass
+    applies the same product, and K is symmetric."""
+    from scipy.signal import butter, freqz
+    n = int(nt) + LOWPASS_PADDING
+    b, a = butter(order, 2 * highcut / fn, btype="lowpass", output="ba")
+    _, h = freqz(b, a, worN=n, whole=True)
+    g = np.fft.ifft(np.conjugate(h) * h).real
+    idx = (np.arange(nt)[:, None] - np.arange(nt)[None, :]) % n
+    return np.ascontiguousarray(g[idx], np.float32)
+
+
+def _device_response(nt, highcut, fn, order, device):
+    import torch
+    key = (int(nt), float(highcut), float(fn), int(order), str(device))
+    if key not in _RESPONSES:
+        _RESPONSES[key] = torch.from_numpy(lowpass_response(nt, highcut, fn, order)).to(device)
+    return _RESPONSES[key]
+
+
+def _filter(x, highcut, fn, order, axis):
+    """Filter (n_planes, nt, ncols) traces along axis 1 on the device
+    (pyfwi_lowpass); numpy in, numpy out (float64, as the reference)."""
+    import torch
+    from . import _native as N
+    from .engine import _ptr, _stream
+    if axis != 1:
+        raise NotImplementedError("the traces are filtered along axis 1 (time), as the FWI driver does")
+    as_numpy = isinstance(x, np.ndarray)
+    t = torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda() if as_numpy else x
+    dev = t.device
+    t = t.to(torch.float32).contiguous()
+    shape = t.shape
+    if t.ndim == 2:  # one plane
+        t = t[None]
+    t = t.reshape(t.shape[0], t.shape[1], -1)  # (planes, nt, traces): '3d' sections too
+    out = torch.empty_like(t)
+    K = _device_response(t.shape[1], highcut, fn, order, dev)
+    N.check(N.lib().pyfwi_lowpass(_ptr(K), _ptr(t), _ptr(out), int(t.shape[1]), int(t.shape[2]), int(t.shape[0]),
+                                  _stream(dev)))
+    out = out.reshape(shape)
+    return out.cpu().numpy().astype(np.float64) if as_numpy else out
+
+
+def lowpass(x1, highcut, fn, order=1, axis=1, show=False):
+    """fwi_tools.py:1188-1222 on the device: the zero-phase Butterworth
+    low-pass of traces (n_planes, nt, ncols) along time."""
+    return _filter(x1, highcut, fn, order, axis)
+
+
+def adj_lowpass(x, highcut, fn, order, axis=1):
+    """fwi_tools.py:1225-1258: the adjoint of lowpass, the same operator."""
+    return _filter(x, highcut, fn, order, axis)
+
+
 def cost_seismic(d_pre0, d_obs0, fun, fn=None, freq=None, order=None, axis=None, sourc_weight=False, ns=None,
                  nr=None, params_oh=None):
-    """Misfit and adjoint source of two data dicts (fwi_tools.py:1290-1345)
-    for the unfiltered case (freq = None)."""
-    if freq:
-        raise NotImplementedError("band-limited misfit (freq) is not provided")
+    """Misfit and adjoint source of two data dicts (fwi_tools.py:1290-1345).
+    With `freq` both data are low-passed (cost_preparation, :1153-1186), the
+    L2 residual is formed, and the adjoint source is the low-passed residual
+    (adj_cost_preparation, :1261-1273).  numpy or torch (device) dicts."""
     if sourc_weight or params_oh is not None:
         raise NotImplementedError("source weighting / parameter weights are not provided")
-    return fun(d_pre0, d_obs0)
+    if not freq:
+        return fun(d_pre0, d_obs0)
+    keys = [k for k in d_pre0]
+    if not all(k in d_obs0 for k in keys):
+        raise KeyError("the observed data miss components of the modelled data")
+    f = lambda d: {k: v for k, v in zip(keys, lowpass(_stack(d, keys), freq, fn, order=order, axis=axis))}
+    rms, res = fun(f(d_pre0), f(d_obs0))
+    adj = adj_lowpass(_stack(res, keys), freq, fn, order=order, axis=axis)
+    if isinstance(adj, np.ndarray):
+        return rms, {k: adj[q].astype(np.float32) for q, k in enumerate(keys)}
+    return rms, {k: adj[q] for q, k in enumerate(keys)}
+
+
+def _stack(d, keys):
+    first = d[keys[0]]
+    if isinstance(first, np.ndarray):
+        return np.stack([np.asarray(d[k], np.float64) for k in keys])
+    import torch
+    return torch.stack([d[k].to(torch.float32) for k in keys])
 
 
 def vel_dict2vec(m0):
