@@ -683,6 +683,39 @@ __global__ void __launch_bounds__(NTHREADS) rev_step(const __grid_constant__ Ste
 // adjoint step + imaging (Adj_injSrc, Adj_update_tau, Adj_update_v, Grad:
 // elastic_surface.cl:48-71, elastic.cl:316-526)
 // ---------------------------------------------------------------------------
+// Differences along a register window w[0..2R] (w[R] is the centre row).
+template <int R, int N>
+__device__ __forceinline__ float wfwd(const float (&w)[N], const float *c)
+{
+    float r = c[0] * (w[R + 1] - w[R]);
+    r = fmaf(c[1], w[R + 2] - w[R - 1], r);
+    if (R == 4) {
+        r = fmaf(c[2], w[R + 3] - w[R - 2], r);
+        r = fmaf(c[3], w[R + 4] - w[R - 3], r);
+    }
+    return r;
+}
+
+template <int R, int N>
+__device__ __forceinline__ float wbwd(const float (&w)[N], const float *c)
+{
+    float r = c[0] * (w[R] - w[R - 1]);
+    r = fmaf(c[1], w[R + 1] - w[R - 2], r);
+    if (R == 4) {
+        r = fmaf(c[2], w[R + 2] - w[R - 3], r);
+        r = fmaf(c[3], w[R + 3] - w[R - 4], r);
+    }
+    return r;
+}
+
+template <int N>
+__device__ __forceinline__ void shift(float (&w)[N], float top)
+{
+#pragma unroll
+    for (int q = 0; q < N - 1; ++q) w[q] = w[q + 1];
+    w[N - 1] = top;
+}
+
 template <int R, int TZ>
 struct AdjShape {
     static constexpr int W = TX + 4 * R;
@@ -808,11 +841,36 @@ __global__ void __launch_bounds__(NTHREADS) adj_step(const __grid_constant__ Adj
     const float *F = a.fwd ? a.fwd + slot * a.fwd_stride : nullptr;
     const __nv_bfloat16 *F16 = a.fwd16 ? a.fwd16 + slot * a.fwd_stride : nullptr;
     float *G = a.gacc + slot * a.gacc_stride;
-    for (int r = tid / TX; r < TZ; r += NTHREADS / TX) {
-        int gi = i0 + r;
+    // each thread takes NK consecutive rows of its column, so the z
+    // differences of the imaging slide down register windows (rows gi-R ..
+    // gi+R of the forward vz, tzz and txz): one new row per field and cell
+    constexpr int NK = TZ / (NTHREADS / TX);
+    const int r0 = (tid / TX) * NK;
+    const long long pz = g.pitch;
+    float wvz[2 * R + 1], wtz[2 * R + 1], wtxz[2 * R + 1];
+    const bool win = F && gj >= glo && gj <= g.tnx - R - a.npml && i0 + r0 + NK - 1 >= glo &&
+                     i0 + r0 <= g.tnz - R - a.npml;
+    if (win) {
+        const long long c0 = cell_off(g, i0 + r0, gj);
+#pragma unroll
+        for (int m = 0; m < 2 * R; ++m) {
+            const long long o = c0 + (m - R) * pz;
+            wvz[m + 1] = __ldg(F + VZ * P + o);
+            wtz[m + 1] = __ldg(F + TZZ * P + o);
+            wtxz[m + 1] = __ldg(F + TXZ * P + o);
+        }
+    }
+    for (int k = 0; k < NK; ++k) {
+        const int r = r0 + k, gi = i0 + r;
         if (gi >= g.tnz) break;
         int is = (r + R) * W + c + 2 * R;
         long long co = cell_off(g, gi, gj);
+        if (win) {  // the window moves to rows gi-R .. gi+R
+            const long long o = co + R * pz;
+            shift(wvz, __ldg(F + VZ * P + o));
+            shift(wtz, __ldg(F + TZZ * P + o));
+            shift(wtxz, __ldg(F + TXZ * P + o));
+        }
         float avx = __ldg(in + VX * P + co), avz = __ldg(in + VZ * P + co);
         if (in_domain(g, R, gi, gj)) {
             float dx = __ldg(a.dampx + gj + XO), dz = __ldg(a.dampz + gi + ZO);
@@ -829,20 +887,20 @@ __global__ void __launch_bounds__(NTHREADS) adj_step(const __grid_constant__ Adj
         float vx = 0.f, vz = 0.f, tx = 0.f, tz = 0.f, txz = 0.f;
         if (F) {
             // DzpVx is formed from vz, as the reference does (elastic.cl:485)
-            dzp_vx = gfwd<R>(F + VZ * P, co, sz_, a.k.cz);
+            dzp_vx = wfwd<R>(wvz, a.k.cz);
             dxm_vz = gbwd<R>(F + VZ * P, co, 1, a.k.cx);
             dxp_vx = gfwd<R>(F + VX * P, co, 1, a.k.cx);
-            dzm_vz = gbwd<R>(F + VZ * P, co, sz_, a.k.cz);
-            dzp_tz = gfwd<R>(F + TZZ * P, co, sz_, a.k.cz);
+            dzm_vz = wbwd<R>(wvz, a.k.cz);
+            dzp_tz = wfwd<R>(wtz, a.k.cz);
             dxm_tx = gbwd<R>(F + TXX * P, co, 1, a.k.cx);
             dxp_txz = gfwd<R>(F + TXZ * P, co, 1, a.k.cx);
-            dzm_txz = gbwd<R>(F + TXZ * P, co, sz_, a.k.cz);
+            dzm_txz = wbwd<R>(wtxz, a.k.cz);
             if (ENERGY) {
                 vx = F[VX * P + co];
-                vz = F[VZ * P + co];
+                vz = wvz[R];
                 tx = F[TXX * P + co];
-                tz = F[TZZ * P + co];
-                txz = F[TXZ * P + co];
+                tz = wtz[R];
+                txz = wtxz[R];
             }
         } else {
 #define B16F(f, k) bf(F16 + (f) * P, (k))

@@ -95,39 +95,6 @@ __device__ __forceinline__ int trow(const float *p, const float *base, int pitch
 // Non-negative ring index of row r for a ring of n rows.
 __device__ __forceinline__ int ring(int r, int n) { return (r % n + n) % n; }
 
-// Differences along a register window w[0..2R] (w[R] is the centre row).
-template <int R, int N>
-__device__ __forceinline__ float wfwd(const float (&w)[N], const float *c)
-{
-    float r = c[0] * (w[R + 1] - w[R]);
-    r = fmaf(c[1], w[R + 2] - w[R - 1], r);
-    if (R == 4) {
-        r = fmaf(c[2], w[R + 3] - w[R - 2], r);
-        r = fmaf(c[3], w[R + 4] - w[R - 3], r);
-    }
-    return r;
-}
-
-template <int R, int N>
-__device__ __forceinline__ float wbwd(const float (&w)[N], const float *c)
-{
-    float r = c[0] * (w[R] - w[R - 1]);
-    r = fmaf(c[1], w[R + 1] - w[R - 2], r);
-    if (R == 4) {
-        r = fmaf(c[2], w[R + 2] - w[R - 3], r);
-        r = fmaf(c[3], w[R + 3] - w[R - 4], r);
-    }
-    return r;
-}
-
-template <int N>
-__device__ __forceinline__ void shift(float (&w)[N], float top)
-{
-#pragma unroll
-    for (int q = 0; q < N - 1; ++q) w[q] = w[q + 1];
-    w[N - 1] = top;
-}
-
 // z-differences down column `col` of a ring whose rows r-R .. r+R start at
 // the offsets o[0..2R] (o[R] is row r).
 template <int R>
