@@ -201,3 +201,22 @@ def test_misfit_gradient_matches_separate_calls(name, extra):
     # the modelled traces are those of forward_modeling
     for k, v in W2.seismogram.items():
         assert np.array_equal(v, W.seismogram[k]), k
+
+
+def test_graph_replay_matches_direct_launches():
+    """inpa['graph'] = True captures each forward / gradient call as a CUDA
+    graph on first use and replays it after: same bits as direct launches,
+    also when the model changes between calls (set_model is not captured)."""
+    import torch
+    case = cases.tiny_dtscale()
+    g = load_golden("tiny_dtscale")
+    res = l2_residual_np(_golden_section(g, "d_est_"), _golden_section(g, "d_obs_"))
+    scaled = {k: (v * np.float32(1.02)) for k, v in case["model_est"].items()}
+    direct, replay = product(case), product(case, graph=True)
+    for model in (case["model_est"], case["model_est"], scaled):
+        a = direct.forward_modeling(model), direct.gradient(res, parameterization="dv")
+        b = replay.forward_modeling(model), replay.gradient(res, parameterization="dv")
+        torch.cuda.synchronize()
+        for da, db in zip(a, b):
+            for k in da:
+                assert np.array_equal(da[k], db[k]), k

@@ -136,3 +136,12 @@ def test_ctypes_structs_follow_the_header(native, cname, pyname):
     """The ctypes mirrors list the header's fields in the header's order."""
     fields = [f[0] for f in getattr(native, pyname)._fields_]
     assert fields == _struct_fields(cname)
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """Without libpyfwi_b200.so there is no compute path: loading raises."""
+    from pyfwi_b200 import _native
+    monkeypatch.setattr(_native, "LIB_PATH", str(tmp_path / "absent.so"))
+    monkeypatch.setattr(_native, "_lib", None)
+    with pytest.raises(ImportError):
+        _native.lib()
