@@ -745,7 +745,7 @@ __device__ __forceinline__ void inject_epilogue(const AdjArgs &a, int slot, int 
 }
 
 template <int R, int TZ, bool ENERGY>
-__global__ void __launch_bounds__(NTHREADS) adj_step(const __grid_constant__ AdjArgs a)
+__global__ void __launch_bounds__(NTHREADS, (R == 2 && !ENERGY) ? 6 : 1) adj_step(const __grid_constant__ AdjArgs a)
 {
     using S = AdjShape<R, TZ>;
     constexpr int W = S::W, HT = S::HT, HV = S::HV, VW = TX + 2 * R;
