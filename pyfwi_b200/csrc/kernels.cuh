@@ -134,6 +134,34 @@ __device__ __forceinline__ float dbwd_p(const float *a, const float *b, int i, i
 #undef P_
 }
 
+// Normal-stress pair of update_tauz (elastic.cl:235-270): txx gains
+// dt ((lam + 2 mu) a + lam b), tzz gains dt (lam a + (lam + 2 mu) b), a = Dx+ vx,
+// b = Dz- vz, then both are damped (forward, coeff = +1; the reverse step,
+// coeff = -1, damps first and subtracts).  Every rounding is spelled out so
+// that where mu = 0 (a fluid) the two increments are the same float: the
+// fluid has no restoring force on txx - tzz, so a rounding difference between
+// them (left to the compiler's choice of fused multiply-adds) would never
+// radiate away and would grow step by step into the velocities.
+__device__ __forceinline__ void normal_pair_fwd(float l, float m, float a, float b, float d, float dt, float &txx,
+                                                float &tzz)
+{
+    const float l2m = l + 2.f * m;
+    txx = __fmaf_rn(dt, __fmaf_rn(l2m, a, __fmul_rn(l, b)), txx);
+    tzz = __fmaf_rn(dt, __fmaf_rn(l, a, __fmul_rn(l2m, b)), tzz);
+    txx = __fmaf_rn(dt, __fmul_rn(-d, txx), txx);
+    tzz = __fmaf_rn(dt, __fmul_rn(-d, tzz), tzz);
+}
+
+__device__ __forceinline__ void normal_pair_rev(float l, float m, float a, float b, float d, float dt, float &txx,
+                                                float &tzz)
+{
+    const float l2m = l + 2.f * m;
+    txx = __fmaf_rn(-dt, __fmul_rn(d, txx), txx);
+    tzz = __fmaf_rn(-dt, __fmul_rn(d, tzz), tzz);
+    txx = __fmaf_rn(-dt, __fmaf_rn(l2m, a, __fmul_rn(l, b)), txx);
+    tzz = __fmaf_rn(-dt, __fmaf_rn(l, a, __fmul_rn(l2m, b)), tzz);
+}
+
 // Differences of (lam + 2 mu) * A.
 template <int R>
 __device__ __forceinline__ float dfwd_l2m(const float *lam, const float *mu, const float *A, int i, int s,
@@ -547,11 +575,7 @@ __global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ Ste
             float sxx = f4(txx, k), szz = f4(tzz, k), sxz = f4(txz, k);
             if (in_domain(g, R, gi, gj + k)) {
                 const float l = f4(lam, k), m = f4(mu, k), d = f4(dx, k) + dz;
-                const float l2m = l + 2.f * m;
-                sxx = sxx + dt * (l2m * dxp_vx[k] + l * dzm_vz[k]);
-                szz = szz + dt * (l2m * dzm_vz[k] + l * dxp_vx[k]);
-                sxx = sxx + dt * (-d * sxx);
-                szz = szz + dt * (-d * szz);
+                normal_pair_fwd(l, m, dxp_vx[k], dzm_vz[k], d, dt, sxx, szz);
                 sxz = sxz + dt * (m * (dxm_vz[k] + dzp_vx[k]));
                 sxz = sxz + dt * (-d * sxz);
             }
@@ -637,17 +661,14 @@ __global__ void __launch_bounds__(NTHREADS) rev_step(const __grid_constant__ Ste
         if (!in_domain(g, R, gi, gj)) continue;
         int is = r * W + cc + R, iv = is + R * W;
         float d = __ldg(a.dampx + gj + XO) + __ldg(a.dampz + gi + ZO);
-        float lam = s_lam[is], mu = s_mu[is], l2m = lam + 2.f * mu;
+        float lam = s_lam[is], mu = s_mu[is];
         float dxp_vx = dfwd<R>(s_vx, iv, 1, a.k.cx), dzm_vz = dbwd<R>(s_vz, iv, W, a.k.cz);
         float dxm_vz = dbwd<R>(s_vz, iv, 1, a.k.cx), dzp_vx = dfwd<R>(s_vx, iv, W, a.k.cz);
         float txz = s_txz[is];
         txz = txz - dt * (d * txz);
         txz = txz - dt * (mu * (dxm_vz + dzp_vx));
         float txx = s_txx[is], tzz = s_tzz[is];
-        txx = txx - dt * (d * txx);
-        tzz = tzz - dt * (d * tzz);
-        txx = txx - dt * (l2m * dxp_vx + lam * dzm_vz);
-        tzz = tzz - dt * (l2m * dzm_vz + lam * dxp_vx);
+        normal_pair_rev(lam, mu, dxp_vx, dzm_vz, d, dt, txx, tzz);
         s_txx[is] = txx;
         s_tzz[is] = tzz;
         s_txz[is] = txz;

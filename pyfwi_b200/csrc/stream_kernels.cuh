@@ -343,11 +343,7 @@ __global__ void __launch_bounds__(W - 2 * R) fwd_stream(const __grid_constant__ 
                 const float *rvx = s_v + (0 * NV + iv) * T, *rvz = s_v + (1 * NV + iv) * T;
                 float dxp_vx = dfwd<R>(rvx, t, 1, a.k.cx), dzm_vz = wbwd<R>(wvz, a.k.cz);
                 float dxm_vz = dbwd<R>(rvz, t, 1, a.k.cx), dzp_vx = wfwd<R>(wvx, a.k.cz);
-                float l2m = lam + 2.f * mu;
-                txx = txx + dt * (l2m * dxp_vx + lam * dzm_vz);
-                tzz = tzz + dt * (l2m * dzm_vz + lam * dxp_vx);
-                txx = txx + dt * (-d * txx);
-                tzz = tzz + dt * (-d * tzz);
+                normal_pair_fwd(lam, mu, dxp_vx, dzm_vz, d, dt, txx, tzz);
                 txz = txz + dt * (mu * (dxm_vz + dzp_vx));
                 txz = txz + dt * (-d * txz);
             }

@@ -165,7 +165,25 @@ def tiny_both():
                 model_est=est)
 
 
-TINY = [tiny_s8, tiny_dtscale, tiny_chpr, tiny_crosswell, tiny_dxr, tiny_both]
+def tiny_water():
+    """A 6-cell water layer (vs = 0) over a layered solid, as in marine
+    surveys: sources and receivers in the water, pressure recorded, 'dv'
+    gradient."""
+    nz, nx, dh, dt = 32, 40, 2.0, 0.0004
+    inpa = {"dt": dt, "t": _t_for(150, dt), "dh": dh, "npml": 5, "pmlR": 1e-5, "pml_dir": 2, "sdo": 4,
+            "rec_dis": dh, "acq_type": 1}
+    src_loc, rec_loc = _surface(nz, nx, dh, 2, rec_depth=2, src_depth=3, src_x=[12, 27])
+    est = layered_model(nz, nx, 13)
+    obs = perturbed(est, 14)
+    for m in (est, obs):
+        m["vp"][:6] = 1500.0
+        m["vs"][:6] = 0.0
+        m["rho"][:6] = 1000.0
+    return dict(name="tiny_water", inpa=inpa, src_loc=src_loc, rec_loc=rec_loc, fdom=70.0, src_type=0,
+                components=0, chpr=100, n_well_rec=0, param="dv", model_obs=obs, model_est=est)
+
+
+TINY = [tiny_s8, tiny_dtscale, tiny_chpr, tiny_crosswell, tiny_dxr, tiny_both, tiny_water]
 ALL = [c1] + TINY  # cases with golden fixtures
 
 
@@ -231,3 +249,14 @@ def c3(ns=64):
     smooth["rho"] = (310 * smooth["vp"] ** 0.25).astype(np.float32)
     return dict(name="c3", inpa=inpa, src_loc=src_loc, rec_loc=rec_loc, fdom=8.0, src_type=0, components=0,
                 chpr=100, n_well_rec=0, param="dv", model_obs=model, model_est=smooth)
+
+
+def fwi_lbfgs():
+    """The inversion driver on tiny_dxr: FWI(...)(m0, 'lbfgs', iter=[2, 2],
+    freqs=[60, 0], n_params=1, k_0=1, k_end=4), i.e. vp, then vs, then rho,
+    two L-BFGS iterations each, first on data low-passed at 60 Hz, then on
+    the full band."""
+    case = tiny_dxr()
+    case["name"] = "fwi_lbfgs"
+    case["fwi"] = dict(method="lbfgs", iter=[2, 2], freqs=[60, 0], n_params=1, k_0=1, k_end=4)
+    return case
