@@ -2,10 +2,12 @@
 propagator.
 
 Same constructor and ``__call__(m0, method, iter, freqs, n_params, k_0,
-k_end)``; SciPy's conjugate gradient / L-BFGS-B drive ``fprime_single`` as in
-the reference.  Each misfit evaluation runs forward modelling, the L2
-residual and the adjoint gradient on the device; only the model and
-gradient vectors cross to the host for SciPy.  The multiscale frequencies
+k_end)``.  Each misfit evaluation runs forward modelling, the L2 residual
+and the adjoint gradient on the device.  ``lbfgs`` runs the reference's
+L-BFGS-B settings with the model, gradient and history vectors on the
+device (lbfgs.minimize); ``inpa['optimizer'] = 'scipy'`` hands the vectors
+to SciPy's ``fmin_l_bfgs_b`` on the host instead, as the reference does.
+``cg`` is SciPy's ``fmin_cg`` on the host.  The multiscale frequencies
 (`freqs`) low-pass the data on the device (fwi_tools.lowpass).
 Regularisation terms (TV, Tikhonov, prior, parameter relations) are not
 provided: asking for them raises."""
@@ -15,6 +17,7 @@ from scipy.optimize import fmin_cg, fmin_l_bfgs_b
 
 from . import acquisition as acq
 from . import fwi_tools as tools
+from . import lbfgs as device_lbfgs
 from .processing import COMPONENTS, prepare_residual
 from .wave_propagation import WavePropagator
 
@@ -42,10 +45,51 @@ class MemoizeJac:
         return self.jac
 
 
+def observed_on_device(W, d):
+    """Observed data dict -> its nonzero components as float32 device
+    tensors, missing components counted as zero (prepare_residual)."""
+    obs = prepare_residual({k: W._to_device(v) for k, v in d.items()}, 1)
+    return {k: v for k, v in obs.items() if bool(torch.any(v != 0))}
+
+
+def evaluate(W, model, d_obs, sd, freq):
+    """L2 misfit of propagator W's data at `model` against `d_obs` (device
+    dict from observed_on_device) and its (vp, vs, rho) gradient on the
+    device (fwi.py:228-252): forward modelling scaled by `sd`, both data
+    low-passed at `freq` when it is set (cost_seismic), residual, gradient.
+    Returns (float misfit, dict of device gradients)."""
+    if freq:
+        d_est = W.forward_modeling(model, show=False)
+        d_est = {k: sd * v for k, v in d_est.items()}
+        keys = [k for k in COMPONENTS if k in d_est or k in d_obs]
+        like = next(iter(d_est.values()))
+        est = {k: d_est[k] if k in d_est else torch.zeros_like(like) for k in keys}
+        obs = {k: d_obs[k] if k in d_obs else torch.zeros_like(like) for k in keys}
+        rms, adj = tools.cost_seismic(est, obs, fun=tools.CostFunction("l2"), fn=W.fn, freq=freq, order=3, axis=1)
+        return float(rms.item()), W.gradient(adj, parameterization="dv")
+    if sd == 1 and set(d_obs) == set(acq.section_keys(W.components)):
+        # forward, misfit and gradient fused per shot group (same result)
+        rms, grad_dv = W.misfit_gradient(model, d_obs, parameterization="dv")
+        return float(rms.item()), grad_dv
+    d_est = W.forward_modeling(model, show=False)
+    d_est = {k: sd * v for k, v in d_est.items()}
+    rms = torch.zeros((), dtype=torch.float64, device=W.device)
+    adj = {}
+    for k in COMPONENTS:
+        if k in d_est or k in d_obs:
+            est = d_est.get(k, torch.zeros_like(next(iter(d_est.values()))))
+            obs = d_obs.get(k, torch.zeros_like(est))
+            r, res = tools.CostFunction("l2")({k: est}, {k: obs})
+            rms += r
+            adj[k] = res[k]
+    return float(rms.item()), W.gradient(adj, parameterization="dv")
+
+
 class FWI(WavePropagator):
     def __init__(self, d_obs, inpa, src, rec_loc, model_shape, components, chpr, n_well_rec=0,
                  param_functions=None):
         super().__init__(inpa, src, rec_loc, model_shape, n_well_rec=n_well_rec, chpr=chpr, components=components)
+        self._default_params = param_functions is None
         if param_functions is None:
             self.dict2vec = tools.vel_dict2vec
             self.vec2dict = tools.vec2vel_dict
@@ -62,12 +106,26 @@ class FWI(WavePropagator):
             if inpa.get(key):
                 raise NotImplementedError("regularisation '%s' is not provided" % key)
         self.sd = inpa.get("sd", 1.0)
+        self.optimizer = inpa.get("optimizer", "device")
+        if self.optimizer not in ("device", "scipy"):
+            raise ValueError("inpa['optimizer'] is 'device' or 'scipy', not %r" % (self.optimizer,))
         if inpa.get("cost_function_type", "l2") != "l2":
             raise NotImplementedError("only the 'l2' misfit is provided")
         self.grad_coeff = inpa.get("grad_coeff", [1.0, 1.0, 1.0])
         self.n_elements = self.nz * self.nx
-        obs = prepare_residual({k: self._to_device(v) for k, v in d_obs.items()}, 1)
-        self.d_obs = {k: v for k, v in obs.items() if bool(torch.any(v != 0))}
+        self.d_obs = d_obs
+
+    @property
+    def d_obs(self):
+        """Observed data: the nonzero components on the device.  Assigning a
+        dict (numpy or torch, any subset of components) converts it, so the
+        time-lapse drivers can swap vintages as the reference does
+        (tl_fwi.py: ``self.inv_obj.d_obs = self.m_dobs``)."""
+        return self._d_obs
+
+    @d_obs.setter
+    def d_obs(self, d):
+        self._d_obs = observed_on_device(self, d)
 
     def __call__(self, m0, method, iter, freqs, n_params, k_0, k_end):
         m = self.dict2vec(m0)
@@ -105,6 +163,10 @@ class FWI(WavePropagator):
         return mtotal, hist
 
     def lbfgs(self, m0, ITER, freq, n_params=1, k0=1, k_end=2):
+        """L-BFGS over parameters k0, k0 + n_params, ... < k_end in turn, ITER
+        iterations each (fwi.py:197-226), the others held fixed."""
+        if self.optimizer == "device":
+            return self._lbfgs_device(m0, ITER, freq, n_params, k0, k_end)
         n = self.nz * self.nx
         mtotal = np.copy(m0)
         hist = []
@@ -112,49 +174,43 @@ class FWI(WavePropagator):
         for k in np.arange(k0, k_end, n_params):
             m_1, m_opt, m1 = mtotal[:k * n], mtotal[k * n:(k + n_params) * n], mtotal[(k + n_params) * n:]
             m_opt, fopt, _ = fmin_l_bfgs_b(fun, m_opt, fun.derivative, args=(m_1, m1, freq), m=10, factr=1e7,
-                                           pgtol=1e-8, bounds=None, maxfun=15000, maxiter=ITER, disp=None,
+                                           pgtol=1e-8, bounds=None, maxfun=15000, maxiter=ITER,
                                            callback=None, maxls=10)
             hist.append(fopt)
             mtotal = np.hstack((m_1, m_opt, m1))
         return mtotal, hist
 
+    def _lbfgs_device(self, m0, ITER, freq, n_params, k0, k_end):
+        n = self.nz * self.nx
+        mtotal = torch.from_numpy(np.asarray(m0, np.float64)).to(self.device)
+        hist = []
+        for k in np.arange(k0, k_end, n_params):
+            m_1, m_opt, m1 = mtotal[:k * n], mtotal[k * n:(k + n_params) * n], mtotal[(k + n_params) * n:]
+            res = device_lbfgs.minimize(lambda x: self.fprime_single(x, m_1, m1, freq), m_opt, m=10, factr=1e7,
+                                        pgtol=1e-8, maxfun=15000, maxiter=ITER, maxls=10)
+            hist.append(res.f)
+            mtotal = torch.cat((m_1, res.x, m1))
+        return mtotal.cpu().numpy(), hist
+
     def fprime(self, m0, freq):
         """Misfit and its gradient (as a vector) at model vector m0; with
-        `freq` both data are low-passed first (cost_seismic, fwi.py:238-240)."""
-        m_old = self.vec2dict(np.copy(m0), self.nz, self.nx)
+        `freq` both data are low-passed first (cost_seismic, fwi.py:238-240).
+        A device tensor m0 gives a device gradient."""
+        if isinstance(m0, torch.Tensor) and not self._default_params:
+            # user parameter functions work on numpy vectors, as in the reference
+            rms, grad = self.fprime(m0.cpu().numpy(), freq)
+            return rms, torch.from_numpy(grad).to(m0.device)
+        m_old = self.vec2dict(m0.clone() if isinstance(m0, torch.Tensor) else np.copy(m0), self.nz, self.nx)
         m_new = self.model_to_dv(m_old, self.param_functions_args)
         model = {k: self._to_device(m_new[k]) for k in ("vp", "vs", "rho")}
-        if freq:
-            d_est = self.forward_modeling(model, show=False)
-            d_est = {k: self.sd * v for k, v in d_est.items()}
-            keys = [k for k in COMPONENTS if k in d_est or k in self.d_obs]
-            like = next(iter(d_est.values()))
-            est = {k: d_est[k] if k in d_est else torch.zeros_like(like) for k in keys}
-            obs = {k: self.d_obs[k] if k in self.d_obs else torch.zeros_like(like) for k in keys}
-            rms, adj = tools.cost_seismic(est, obs, fun=tools.CostFunction("l2"), fn=self.fn, freq=freq, order=3,
-                                          axis=1)
-            return self._finish(float(rms.item()), self.gradient(adj, parameterization="dv"), m_old)
-        if self.sd == 1 and set(self.d_obs) == set(acq.section_keys(self.components)):
-            # forward, misfit and gradient fused per shot group (same result)
-            rms, grad_dv = self.misfit_gradient(model, self.d_obs, parameterization="dv")
-            return self._finish(float(rms.item()), grad_dv, m_old)
-        d_est = self.forward_modeling(model, show=False)
-        d_est = {k: self.sd * v for k, v in d_est.items()}
-        rms = torch.zeros((), dtype=torch.float64, device=self.device)
-        adj = {}
-        for k in COMPONENTS:
-            if k in d_est or k in self.d_obs:
-                est = d_est.get(k, torch.zeros_like(next(iter(d_est.values()))))
-                obs = self.d_obs.get(k, torch.zeros_like(est))
-                r, res = tools.CostFunction("l2")({k: est}, {k: obs})
-                rms += r
-                adj[k] = res[k]
-        grad_dv = self.gradient(adj, parameterization="dv")
-        return self._finish(float(rms.item()), grad_dv, m_old)
+        rms, grad_dv = evaluate(self, model, self.d_obs, self.sd, freq)
+        return self._finish(rms, grad_dv, m_old)
 
     def _finish(self, rms, grad_dv, m_old):
-        """Gradient vector from the (vp, vs, rho) device gradient (fwi.py:243-252)."""
-        grad_dv = {k: v.cpu().numpy() for k, v in grad_dv.items()}
+        """Gradient vector from the (vp, vs, rho) device gradient (fwi.py:243-252),
+        on the device when the model vector was."""
+        if not isinstance(m_old["vp"], torch.Tensor):
+            grad_dv = {k: v.cpu().numpy() for k, v in grad_dv.items()}
         grad = self.grad_from_dv(grad_dv, self.param_functions_args, m_old)
         params = [*grad]
         for q in range(3):
@@ -162,7 +218,13 @@ class FWI(WavePropagator):
         return rms, self.dict2vec(grad)
 
     def fprime_single(self, m0, m_1, m1, freq):
-        mtotal = np.float32(np.hstack((m_1, m0, m1)))
-        s1, s0 = np.shape(m_1)[0], np.shape(m0)[0]
+        """Misfit and gradient of the parameters in m0, the others (m_1
+        before, m1 after) fixed; the model is rounded to float32 first
+        (fwi.py:255-259)."""
+        if isinstance(m0, torch.Tensor):
+            mtotal = torch.cat((m_1, m0, m1)).to(torch.float32)
+        else:
+            mtotal = np.float32(np.hstack((m_1, m0, m1)))
+        s1, s0 = m_1.shape[0], m0.shape[0]
         rms, grad = self.fprime(mtotal, freq)
         return rms, grad[s1:s1 + s0]

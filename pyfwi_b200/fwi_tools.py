@@ -203,7 +203,11 @@ def _stack(d, keys):
 
 
 def vel_dict2vec(m0):
-    """(vp, vs, rho) dict -> one vector (fwi_tools.py:1066-1073)."""
+    """(vp, vs, rho) dict -> one float64 vector (fwi_tools.py:1066-1073);
+    torch tensors give a tensor on their device."""
+    import torch
+    if isinstance(m0["vp"], torch.Tensor):
+        return torch.cat([m0[k].reshape(-1).to(torch.float64) for k in ("vp", "vs", "rho")])
     nz, nx = m0[[*m0][0]].shape
     m = np.zeros((3 * nz * nx))
     m[:nz * nx] = m0["vp"].reshape(-1)

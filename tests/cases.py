@@ -251,6 +251,47 @@ def c3(ns=64):
                 chpr=100, n_well_rec=0, param="dv", model_obs=model, model_est=smooth)
 
 
+def c4(n_models=32, seed=44):
+    """The uneven batch: n_models seeded surveys, each a layered model (vp
+    1500 -> 4500 m/s with depth, 2-4 dipping layers) with one anomaly (+-8 %
+    disc), vs = vp / 1.8, Gardner rho; grid nz in [128, 512], nx in [128,
+    1024], dh in [2, 10] m, 20-cell layer; dt = 0.5 dh / max(vp) (CFL 0.5;
+    above 0.6 ms the propagator sub-steps); nt in [1000, 5000]; 4-16
+    explosive shots at 2 cells depth and a receiver in every column at 2
+    cells; f0 = min(vs) / (16 dh) clipped to [5, 30] Hz (at least 8 cells per
+    wavelength at twice f0); vx and vz recorded, every step checkpointed.
+    The estimate is the model smoothed (8-cell Gaussian)."""
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n_models):
+        nz, nx = int(rng.integers(128, 513)), int(rng.integers(128, 1025))
+        dh = float(rng.uniform(2.0, 10.0))
+        z = np.arange(nz)[:, None] / (nz - 1)
+        x = np.arange(nx)[None, :] / (nx - 1)
+        vp = 1500.0 + 2200.0 * z + 0 * x
+        for _ in range(int(rng.integers(2, 5))):
+            z0, slope, jump = rng.uniform(0.15, 0.85), rng.uniform(-0.2, 0.2), rng.uniform(-150, 250)
+            vp = vp + jump * (z > z0 + slope * (x - 0.5))
+        cz, cx, r = rng.uniform(0.3, 0.7), rng.uniform(0.2, 0.8), rng.uniform(0.05, 0.15)
+        disc = ((z - cz) * nz) ** 2 + ((x - cx) * nx) ** 2 < (r * min(nz, nx)) ** 2
+        vp = np.clip(np.where(disc, vp * (1 + rng.choice([-0.08, 0.08])), vp), 1500.0, 4500.0).astype(np.float32)
+        model = {"vp": vp, "vs": (vp / 1.8).astype(np.float32), "rho": (310 * vp ** 0.25).astype(np.float32)}
+        est = {"vp": gaussian_filter(vp, 8.0).astype(np.float32)}
+        est["vs"] = (est["vp"] / 1.8).astype(np.float32)
+        est["rho"] = (310 * est["vp"] ** 0.25).astype(np.float32)
+        dt = float(np.float32(0.5 * dh / float(vp.max())))
+        nt = int(rng.integers(1000, 5001))
+        ns = int(rng.integers(4, 17))
+        f0 = float(np.clip(float(model["vs"].min()) / (16 * dh), 5.0, 30.0))
+        inpa = {"dt": dt, "t": _t_for(nt, dt), "dh": dh, "npml": 20, "pmlR": 1e-5, "pml_dir": 2, "sdo": 4,
+                "rec_dis": dh, "acq_type": 1}
+        src_loc, rec_loc = _surface(nz, nx, dh, ns, rec_depth=2, src_depth=2)
+        out.append(dict(name="c4_%02d" % q, inpa=inpa, src_loc=src_loc, rec_loc=rec_loc, fdom=f0, src_type=0,
+                        components=2, chpr=100, n_well_rec=0, param="dv", model_obs=model, model_est=est))
+    return out
+
+
 def fwi_lbfgs():
     """The inversion driver on tiny_dxr: FWI(...)(m0, 'lbfgs', iter=[2, 2],
     freqs=[60, 0], n_params=1, k_0=1, k_end=4), i.e. vp, then vs, then rho,
@@ -260,3 +301,20 @@ def fwi_lbfgs():
     case["name"] = "fwi_lbfgs"
     case["fwi"] = dict(method="lbfgs", iter=[2, 2], freqs=[60, 0], n_params=1, k_0=1, k_end=4)
     return case
+
+
+def timelapse(method):
+    """Time-lapse inversion on tiny_dxr: baseline = the case's observed
+    model, monitor = baseline with vp -8 % in a 6 x 8-cell patch (a depleted
+    reservoir), start = the case's estimate; TimeLapse(...)(m0, iter=[1],
+    freqs=[60], tl_method=method, n_params=1, k_0=1, k_end=3): vp, then vs."""
+    case = tiny_dxr()
+    case["name"] = "tl_" + method
+    mon = {k: v.copy() for k, v in case["model_obs"].items()}
+    mon["vp"][14:20, 15:23] *= np.float32(0.92)
+    case["model_mon"] = mon
+    case["tl"] = dict(tl_method=method, iter=[1], freqs=[60], n_params=1, k_0=1, k_end=3)
+    return case
+
+
+TL_METHODS = ["cc", "dd", "sim"]
