@@ -303,10 +303,11 @@ def run_ours(args, world, rank, local):
     layout = {"checkpoint": W.checkpoint, "segment": W.segment, "shot_batch": W.shot_batch,
               "kernels": {"forward": int(W.tile), "adjoint": int(W.adj_tile)}}
     plain = None
-    if world == 1 and args.plain_shots > 0:
+    if world == 1 and (args.plain_shots > 0 or args.inversion > 0 or args.uneven > 0):
         del step, W, d_obs, g, rms
         gc.collect()
         torch.cuda.empty_cache()
+    if world == 1 and args.plain_shots > 0:
         plain = plain_form(args, dev, batched_shots_s)
     hbm, peak_src = peaks()
     # dominant kernel: the one with the most device time
@@ -330,6 +331,16 @@ def run_ours(args, world, rank, local):
             "launches": n_l, "avg_launch_ms": ms_k / max(n_l, 1),
             "alg_bytes_per_launch": alg_bytes / max(n_l, 1),
             "kernel_share": {kinds[k][0]: prof[k][1] / max(ms, 1e-9) for k in prof}}
+    uneven = None
+    if world == 1 and args.uneven > 0:
+        gc.collect()
+        torch.cuda.empty_cache()
+        uneven = uneven_run(args, dev)
+    inversion = None
+    if world == 1 and args.inversion > 0:
+        gc.collect()
+        torch.cuda.empty_cache()
+        inversion = {opt: inversion_run(args, case, dev, opt) for opt in ("device", "scipy")}
     cpu = None
     if world == 1 and not args.no_cpu:
         v, kind, cores, desc = cpu_sample(survey(1), seconds=args.cpu_seconds)
@@ -344,7 +355,95 @@ def run_ours(args, world, rank, local):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "clocks": clocks,
             "misfit": misfit}
+    if inversion:
+        line["inversion"] = inversion
+    if uneven:
+        line["uneven_batch"] = uneven
     print(json.dumps(line), flush=True)
+
+
+def inversion_run(args, case, dev, optimizer):
+    """`args.inversion` L-BFGS iterations of FWI on vp through the public
+    driver (FWI.__call__, full band) with the optimiser on the device or
+    SciPy's on the host: wall time per evaluation, and the wall time of the
+    whole call outside the evaluations (the optimiser, the model and
+    gradient vectors, the conversions at entry and exit)."""
+    import torch
+    from helpers import product
+    from pyfwi_b200 import acquisition as acq
+    from pyfwi_b200.fwi import FWI
+    inpa = dict(case["inpa"], cuda_device=str(dev), optimizer=optimizer)
+    src = acq.Source(case["src_loc"], inpa["dh"], inpa["dt"], case["src_type"])
+    src.Ricker(case["fdom"])
+    shape = case["model_est"]["vp"].shape
+    kw = dict(components=case["components"], n_well_rec=case["n_well_rec"], chpr=case["chpr"])
+    W = product(case, cuda_device=str(dev))
+    d_obs = {k: v.clone() for k, v in W.forward_modeling(
+        {k: torch.from_numpy(v).to(dev) for k, v in case["model_obs"].items()}).items()}
+    del W
+    gc.collect()
+    F = FWI(d_obs, inpa, src, case["rec_loc"], shape, **kw)
+    spent = [0.0, 0]
+    inner = F.fprime
+
+    def timed(m0, freq):
+        t0 = time.perf_counter()
+        out = inner(m0, freq)
+        torch.cuda.synchronize()
+        spent[0] += time.perf_counter() - t0
+        spent[1] += 1
+        return out
+    F.fprime = timed
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    F({k: v.copy() for k, v in case["model_est"].items()}, "lbfgs", iter=[args.inversion], freqs=[0], n_params=1,
+      k_0=1, k_end=2)
+    total = time.perf_counter() - t0
+    return {"iterations": args.inversion, "evaluations": spent[1], "s_per_evaluation": spent[0] / spent[1],
+            "outside_evaluations_ms": (total - spent[0]) * 1e3, "parameters": int(np.prod(shape)),
+            "layout": {"segment": F.segment, "shot_batch": F.shot_batch}}
+
+
+def uneven_run(args, dev):
+    """The uneven batch (`args.uneven` surveys of cases.c4): one misfit and
+    gradient evaluation of every survey, (1) one survey after another, (2)
+    together on per-survey streams (SurveyBatch), (3) as one CUDA graph
+    (SurveyBatch(graph=True)); device time and Gcell-updates/s of each,
+    after one untimed evaluation."""
+    import cases
+    import torch
+    from helpers import product
+    from pyfwi_b200.batch import SurveyBatch
+    cs = cases.c4(args.uneven)
+    props = [product(c, cuda_device=str(dev)) for c in cs]
+    batch = SurveyBatch(props)  # shares the device memory out before any plan is built
+    models, observed = [], []
+    for W, c in zip(props, cs):
+        m_obs = {k: torch.from_numpy(v).to(dev) for k, v in c["model_obs"].items()}
+        observed.append({k: v.clone() for k, v in W.forward_modeling(m_obs).items()})
+        models.append({k: torch.from_numpy(v).to(dev) for k, v in c["model_est"].items()})
+    cells = sum(2.0 * int(W.tnz) * int(W.tnx) * int(W.nt) * int(W.ns) for W in props)
+
+    def sequential():
+        for W, m, o in zip(props, models, observed):
+            W.misfit_gradient(m, o, parameterization="dv")
+
+    graphed = SurveyBatch(props, graph=True)
+    forms = {"sequential": sequential,
+             "streams": lambda: batch.misfit_gradient(models, observed),
+             "graph": lambda: graphed.misfit_gradient(models, observed)}
+    out = {"surveys": len(props), "cell_updates": cells}
+    for name, fn in forms.items():
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[name] = {"ms": ms, "value": cells / (ms * 1e-3) / 1e9, "unit": UNIT}
+    return out
 
 
 def plain_form(args, dev, batched_shots_s):
@@ -402,6 +501,10 @@ def main():
     ap.add_argument("--adj-tile", type=int, default=None, help="adjoint step kernel variant when it differs")
     ap.add_argument("--plain-shots", type=int, default=2,
                     help="shots of the plain one-shot-per-launch form timed beside the batched one (0: skip)")
+    ap.add_argument("--inversion", type=int, default=0,
+                    help="also time this many L-BFGS iterations of FWI (device and host optimiser)")
+    ap.add_argument("--uneven", type=int, default=0,
+                    help="also time a batch of this many uneven-size surveys (sequential, streams, graph)")
     args = ap.parse_args()
     if args.impl == "reference":
         # rank 0 alone times the host CPU; other ranks have nothing to do

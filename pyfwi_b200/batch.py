@@ -4,7 +4,10 @@
 different grids, record lengths, shot counts and receiver layouts — together
 on one GPU.  Each survey's plan runs on its own CUDA stream, so the step
 kernels of small surveys overlap instead of leaving the GPU idle between
-launches.  With ``graph=True`` the whole batch (every survey's forward,
+launches.  Surveys whose plans are not built yet share the free device
+memory in proportion to their every-step storage (cells x steps x shots),
+so the first survey's layout does not take the memory the others need.
+With ``graph=True`` the whole batch (every survey's forward,
 residual and adjoint) is captured once into a single CUDA graph and each
 later evaluation is one graph launch; models and observed data are copied
 into the captured buffers first.
@@ -13,6 +16,7 @@ The reference evaluates one survey at a time (one ``WavePropagator`` per
 model, wave_propagation.py:594-938); results here are the same as evaluating
 each survey alone with ``WavePropagator.misfit_gradient``.
 """
+import numpy as np
 import torch
 
 from .engine import require_cuda
@@ -29,10 +33,31 @@ class SurveyBatch:
         if any(torch.device(W.device) != self.device for W in self.props):
             raise ValueError("every survey of a batch must be on one device")
         self.streams = [torch.cuda.Stream(self.device) for _ in self.props]
+        self._share_memory()
         self.graph = graph
         self._graph = None
         self._inputs = None
         self._outputs = None
+
+    def _share_memory(self, fraction=0.8):
+        """Device memory caps for the surveys whose plans are not built:
+        each gets its fixed need (the trace buffers the layout reserves, a
+        recompute store of about 2 sqrt(nt) states of one shot, 256 MB) and a
+        share of the rest in proportion to its every-step storage."""
+        todo = [W for W in self.props if W._plan is None and W.memory_budget is None]
+        if len(todo) < 2:
+            return
+        free, _ = torch.cuda.mem_get_info(self.device)
+        free += torch.cuda.memory_reserved(self.device) - torch.cuda.memory_allocated(self.device)
+        fixed, var = [], []
+        for W in todo:
+            state = 20.0 * int(W.tnz) * int(W.tnx)  # five float32 fields
+            traces = 5.0 * int(W.nt_ext) * int(W.ns) * int(W.nr) * 4
+            fixed.append(4 * traces + (2 * int(np.ceil(np.sqrt(int(W.nt)))) + 8) * state + (256 << 20))
+            var.append(state * int(W.nt) * int(W.ns))
+        spare = max(fraction * free - sum(fixed), 0.0)
+        for W, f, v in zip(todo, fixed, var):
+            W.memory_budget = int(f + spare * v / sum(var))
 
     def _run(self, models, observed, param):
         out = [None] * len(self.props)

@@ -127,6 +127,9 @@ class WavePreparation:
         self._wavelet = self._source_values()
         self._plan = None  # built on first use (device memory is sized then)
         self._traces = None
+        # cap in bytes on the device memory the layout may plan for (None:
+        # what is free when the plan is built); SurveyBatch shares memory out
+        self.memory_budget = None
 
     @property
     def plan(self):
@@ -323,6 +326,11 @@ class WavePreparation:
         few shots beats recomputing a large batch only where the grid is large
         enough to fill the GPU with a few shots."""
         free, _ = torch.cuda.mem_get_info(self.device)
+        # blocks torch's caching allocator holds but does not use count as
+        # free: it releases them when an allocation would otherwise fail
+        free += torch.cuda.memory_reserved(self.device) - torch.cuda.memory_allocated(self.device)
+        if self.memory_budget is not None:
+            free = min(free, int(self.memory_budget / 0.9))
         traces = 5 * self.nt_ext * int(self.ns) * int(self.nr) * 4
         budget = int(0.9 * free) - 4 * traces - (256 << 20)
         nt, ns = int(self.nt), int(self.ns)
