@@ -144,7 +144,7 @@ def cpu_sample(case, seconds=15.0, max_steps=4000):
         R = ref_driver.RefRunner(case["name"], W)
         probe = 16
         t = R.run_shot(0, probe)
-        n = int(min(max_steps, max(probe, seconds / (t / probe))))
+        n = int(min(max_steps, int(W.nt), max(probe, seconds / (t / probe))))
         t = R.run_shot(0, n)
         kind = "reference"
         desc = ("PyFWI elastic.cl/elastic_surface.cl compiled for the host (OpenMP, %d threads), reference loop "
@@ -170,7 +170,7 @@ def cpu_sample(case, seconds=15.0, max_steps=4000):
             return time.perf_counter() - t0
 
         t = run(probe)
-        n = int(min(max_steps, max(probe, seconds / (t / probe))))
+        n = int(min(max_steps, int(W.nt), max(probe, seconds / (t / probe))))
         t = run(n)
         kind = "port"
         desc = ("oracle restatement (C, OpenMP, %d threads), 1 shot x first %d of %d steps, forward + backward"
@@ -303,7 +303,7 @@ def run_ours(args, world, rank, local):
     layout = {"checkpoint": W.checkpoint, "segment": W.segment, "shot_batch": W.shot_batch,
               "kernels": {"forward": int(W.tile), "adjoint": int(W.adj_tile)}}
     plain = None
-    if world == 1 and (args.plain_shots > 0 or args.inversion > 0 or args.uneven > 0):
+    if world == 1 and (args.plain_shots > 0 or args.inversion > 0 or args.uneven > 0 or args.configs):
         del step, W, d_obs, g, rms
         gc.collect()
         torch.cuda.empty_cache()
@@ -331,6 +331,11 @@ def run_ours(args, world, rank, local):
             "launches": n_l, "avg_launch_ms": ms_k / max(n_l, 1),
             "alg_bytes_per_launch": alg_bytes / max(n_l, 1),
             "kernel_share": {kinds[k][0]: prof[k][1] / max(ms, 1e-9) for k in prof}}
+    small = None
+    if world == 1 and args.configs:
+        gc.collect()
+        torch.cuda.empty_cache()
+        small = configs_run(args, dev)
     uneven = None
     if world == 1 and args.uneven > 0:
         gc.collect()
@@ -359,6 +364,8 @@ def run_ours(args, world, rank, local):
         line["inversion"] = inversion
     if uneven:
         line["uneven_batch"] = uneven
+    if small:
+        line["configs"] = small
     print(json.dumps(line), flush=True)
 
 
@@ -408,8 +415,9 @@ def uneven_run(args, dev):
     """The uneven batch (`args.uneven` surveys of cases.c4): one misfit and
     gradient evaluation of every survey, (1) one survey after another, (2)
     together on per-survey streams (SurveyBatch), (3) as one CUDA graph
-    (SurveyBatch(graph=True)); device time and Gcell-updates/s of each,
-    after one untimed evaluation."""
+    (SurveyBatch(graph=True)), (4) one after another with plans that replay
+    their own captured graphs (inpa['graph']); device time and
+    Gcell-updates/s of each, after one untimed evaluation."""
     import cases
     import torch
     from helpers import product
@@ -433,7 +441,8 @@ def uneven_run(args, dev):
              "streams": lambda: batch.misfit_gradient(models, observed),
              "graph": lambda: graphed.misfit_gradient(models, observed)}
     out = {"surveys": len(props), "cell_updates": cells}
-    for name, fn in forms.items():
+
+    def timed(name, fn):
         fn()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -443,6 +452,58 @@ def uneven_run(args, dev):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         out[name] = {"ms": ms, "value": cells / (ms * 1e-3) / 1e9, "unit": UNIT}
+    for name, fn in forms.items():
+        timed(name, fn)
+    # (4) one survey after another again, each plan replaying its own
+    # captured graph (inpa['graph'] = True)
+    del forms, batch, graphed, props
+    gc.collect()
+    torch.cuda.empty_cache()
+    props = [product(c, cuda_device=str(dev), graph=True) for c in cs]
+    SurveyBatch(props)  # memory shares only
+
+    def sequential_graphs():
+        for W, m, o in zip(props, models, observed):
+            W.misfit_gradient(m, o, parameterization="dv")
+    timed("sequential_graph_plans", sequential_graphs)
+    return out
+
+
+def configs_run(args, dev):
+    """The two smaller configurations (cases.c1: 100 x 100 cells, 4 shots,
+    nt 500; cases.c2: 200 x 400 cells, 10 shots, nt 2000): one misfit and
+    gradient evaluation of all shots on the device (CUDA events, 3 timed
+    after 1 untimed), and the reference's kernels on the host cores on one
+    shot (bounded sample, as cpu_baseline); Gcell-updates/s and shots/s."""
+    import cases
+    import torch
+    from helpers import product
+    out = {}
+    for name in ("c1", "c2"):
+        case = cases.by_name(name)
+        W = product(case, cuda_device=str(dev))
+        obs = {k: v.clone() for k, v in W.forward_modeling(
+            {k: torch.from_numpy(v).to(dev) for k, v in case["model_obs"].items()}).items()}
+        model = {k: torch.from_numpy(v).to(dev) for k, v in case["model_est"].items()}
+        per_shot = 2.0 * int(W.tnz) * int(W.tnx) * int(W.nt)
+        W.misfit_gradient(model, obs)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            W.misfit_gradient(model, obs)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        gpu = {"ms_per_evaluation": ms, "value": per_shot * int(W.ns) / (ms * 1e-3) / 1e9, "unit": UNIT,
+               "shots_per_s": int(W.ns) / (ms * 1e-3)}
+        del W, obs
+        cpu = None
+        if not args.no_cpu:
+            v, kind, cores, desc = cpu_sample(case, seconds=args.cpu_seconds / 3)
+            cpu = {"value": v, "unit": UNIT, "shots_per_s": v * 1e9 / per_shot, "cores": cores, "kind": kind,
+                   "sample": desc}
+        out[name] = {"gpu": gpu, "cpu": cpu}
     return out
 
 
@@ -505,6 +566,8 @@ def main():
                     help="also time this many L-BFGS iterations of FWI (device and host optimiser)")
     ap.add_argument("--uneven", type=int, default=0,
                     help="also time a batch of this many uneven-size surveys (sequential, streams, graph)")
+    ap.add_argument("--configs", action="store_true",
+                    help="also time the 100 x 100 and 200 x 400 configurations (device and host reference)")
     args = ap.parse_args()
     if args.impl == "reference":
         # rank 0 alone times the host CPU; other ranks have nothing to do

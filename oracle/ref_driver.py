@@ -80,6 +80,10 @@ class RefRunner:
         """Forward over steps [0, nsteps) storing every state, then the
         backward loop over t = nsteps-1 .. 1.  Returns seconds spent."""
         W, g = self.W, self.g
+        if not 0 < nsteps <= int(W.nt):
+            # the reference's trace buffers hold nt_ext rows: more steps would
+            # write past them
+            raise ValueError("nsteps must be in [1, %d], not %d" % (int(W.nt), nsteps))
         t0 = time.perf_counter()
         for b in self.f:
             b.v[:] = 0

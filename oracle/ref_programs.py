@@ -17,7 +17,7 @@ import cases  # noqa: E402
 import oracle as O  # noqa: E402
 import ref_build  # noqa: E402
 
-BASELINE_CASES = ["c1", "c3"]
+BASELINE_CASES = ["c1", "c2", "c3"]
 
 
 def geometry_of(case):

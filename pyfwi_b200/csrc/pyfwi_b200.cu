@@ -100,7 +100,7 @@ struct pyfwi_plan {
         cudaGraphExec_t exec = nullptr;
         std::vector<uintptr_t> key;
         long long launches = 0;
-    } gfwd, ggrad;
+    } gfwd, ggrad, gmis;
     cudaStream_t cap = nullptr;  // capture stream (the caller's may be the legacy default stream)
     // tensor map of the workspace for the streaming kernels, per box width
     struct TMap {
@@ -565,20 +565,22 @@ int launch_exact(pyfwi_plan *p, const ExactArgs &a, int nslots, cudaStream_t s)
 {
     dim3 grid((p->g.tnx + TX - 1) / TX, (p->g.tnz + TZ - 1) / TZ, nslots);
     const size_t sm = ExactShape<R, TZ>::FLOATS * sizeof(float);
-    static bool attr = false;
-    if (!attr) {
-        CK(cudaFuncSetAttribute(exact_adj_step<R, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        attr = true;
+    const int bf = a.s1h != nullptr;
+    auto kern = bf ? exact_adj_step<R, TZ, true> : exact_adj_step<R, TZ, false>;
+    static bool attr[2] = {false, false};
+    if (!attr[bf]) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        attr[bf] = true;
     }
-    exact_adj_step<R, TZ><<<grid, NTHREADS, sm, s>>>(a);
+    kern<<<grid, NTHREADS, sm, s>>>(a);
     p->launches++;
     CKL();
     return PYFWI_OK;
 }
 
-// The exact adjoint of one group (exact checkpoints, FP32 snapshots): for
-// t = nt-1 .. 0 the transposed step from L_{t+1} to L_t with S_{t+1} and S_t
-// from the segment store, then the trace adjoint of step t.
+// The exact adjoint of one group (exact checkpoints): for t = nt-1 .. 0 the
+// transposed step from L_{t+1} to L_t with S_{t+1} and S_t from the segment
+// store (FP32) or the BF16 snapshots, then the trace adjoint of step t.
 int exact_backward(pyfwi_plan *p, void *ws, const float *const *residual, int s0, int n, cudaStream_t st)
 {
     const pyfwi_geometry &G = p->geom;
@@ -606,9 +608,16 @@ int exact_backward(pyfwi_plan *p, void *ws, const float *const *residual, int s0
         const int t_lo = m * p->seg, t_hi = std::min((m + 1) * p->seg, G.nt);
         if (m < p->M - 1) {  // recompute segment m from its restart state
             for (int t = t_lo; t < t_hi; ++t) {
-                Buf out = {store + (long long)(p->M + t - t_lo) * p->state, sstride};
-                Buf in = t > t_lo ? Buf{store + (long long)(p->M + t - t_lo - 1) * p->state, sstride}
-                                  : exact_state(p, ws, t);
+                Buf in = exact_state(p, ws, t), out;
+                if (bf16_snaps(p)) {  // FP32 chain in the work states, BF16 copies into the snapshots
+                    out = work_state(p, ws, (t + 1) & 1);
+                    if (t > t_lo) in = work_state(p, ws, t & 1);
+                    f.snap = snap_at(p, ws, t - t_lo);
+                    f.snap_stride = (long long)p->seg * p->state;
+                } else {
+                    out = {store + (long long)(p->M + t - t_lo) * p->state, sstride};
+                    if (t > t_lo) in = {store + (long long)(p->M + t - t_lo - 1) * p->state, sstride};
+                }
                 f.in = in.base;
                 f.in_stride = in.stride;
                 f.out = out.base;
@@ -621,11 +630,21 @@ int exact_backward(pyfwi_plan *p, void *ws, const float *const *residual, int s0
             }
         }
         for (int t = t_hi - 1; t >= t_lo; --t) {
-            Buf s_t = t > t_lo ? Buf{store + (long long)(p->M + t - t_lo - 1) * p->state, sstride}
-                               : exact_state(p, ws, t);
-            e.s1 = store + (long long)(p->M + t - t_lo) * p->state;
-            e.s0 = s_t.base;
-            e.s0_stride = s_t.stride;
+            if (bf16_snaps(p)) {
+                // snapshot k holds S_{t_lo+k+1}; S_{t_lo} is the FP32 restart state
+                e.s1h = snap_at(p, ws, t - t_lo);
+                e.s1_stride = (long long)p->seg * p->state;
+                e.s0h = t > t_lo ? snap_at(p, ws, t - t_lo - 1) : nullptr;
+                Buf s_t = exact_state(p, ws, t_lo);
+                e.s0 = t > t_lo ? nullptr : s_t.base;
+                e.s0_stride = t > t_lo ? e.s1_stride : s_t.stride;
+            } else {
+                Buf s_t = t > t_lo ? Buf{store + (long long)(p->M + t - t_lo - 1) * p->state, sstride}
+                                   : exact_state(p, ws, t);
+                e.s1 = store + (long long)(p->M + t - t_lo) * p->state;
+                e.s0 = s_t.base;
+                e.s0_stride = s_t.stride;
+            }
             e.add_src = t % G.dt_scale == 0;
             e.src = src_at(p, t / G.dt_scale);
             e.in = adj + (long long)ping * p->state;
@@ -862,11 +881,15 @@ int forward_enqueue(pyfwi_plan *p, void *ws, float *traces, cudaStream_t st)
 
 // Replay `enqueue` as a CUDA graph: captured once per distinct key (the
 // pointers and values the launches bake in) on the plan's own stream, then
-// launched on the caller's stream.
+// launched on the caller's stream.  A caller stream that is being captured
+// already (the caller builds its own graph) gets the launches directly.
 template <typename F>
 int run_graph(pyfwi_plan *p, pyfwi_plan::GraphCache &c, const std::vector<uintptr_t> &key, cudaStream_t st,
               F enqueue)
 {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return enqueue(st);
     if (!c.exec || c.key != key) {
         if (c.exec) {
             cudaGraphExecDestroy(c.exec);
@@ -948,9 +971,8 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
     if (opt->adj_tile < 0 || opt->adj_tile > N_TILES) return fail(PYFWI_E_INVALID, "adj_tile out of range");
     if (opt->adjoint != PYFWI_ADJOINT_REFERENCE && opt->adjoint != PYFWI_ADJOINT_EXACT)
         return fail(PYFWI_E_INVALID, "unknown adjoint kind");
-    if (opt->adjoint == PYFWI_ADJOINT_EXACT &&
-        (opt->checkpoint != PYFWI_CKPT_EXACT || opt->snapshot != PYFWI_SNAP_FP32 || opt->energy))
-        return fail(PYFWI_E_INVALID, "the exact adjoint needs exact checkpoints, FP32 snapshots and no energy terms");
+    if (opt->adjoint == PYFWI_ADJOINT_EXACT && (opt->checkpoint != PYFWI_CKPT_EXACT || opt->energy))
+        return fail(PYFWI_E_INVALID, "the exact adjoint needs exact checkpoints and no energy terms");
     if (opt->chunk < 0) return fail(PYFWI_E_INVALID, "chunk must be >= 0");
 
     pyfwi_plan *p = new pyfwi_plan();
@@ -1052,6 +1074,7 @@ int pyfwi_plan_destroy(pyfwi_plan *plan)
         }
         if (plan->gfwd.exec) cudaGraphExecDestroy(plan->gfwd.exec);
         if (plan->ggrad.exec) cudaGraphExecDestroy(plan->ggrad.exec);
+        if (plan->gmis.exec) cudaGraphExecDestroy(plan->gmis.exec);
         if (plan->cap) cudaStreamDestroy(plan->cap);
     }
     delete plan;
@@ -1231,7 +1254,22 @@ int pyfwi_misfit_gradient(pyfwi_plan *p, void *ws, size_t bytes, const float *sr
         return fail(PYFWI_E_INVALID, "mean_stress needs adjoint buffers for both stress fields");
     p->src_vals.assign(src_vals, src_vals + 4 * (size_t)n_src);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    rc = gradient_enqueue(p, ws, nullptr, param, grad, nullptr, st, &mf);
+    std::vector<uintptr_t> key = {reinterpret_cast<uintptr_t>(ws), reinterpret_cast<uintptr_t>(traces),
+                                  reinterpret_cast<uintptr_t>(grad), reinterpret_cast<uintptr_t>(misfit),
+                                  (uintptr_t)param, (uintptr_t)mf.mean_stress, (uintptr_t)p->fwd_valid};
+    for (int c = 0; c < 5; ++c) {
+        key.push_back(reinterpret_cast<uintptr_t>(observed[c]));
+        key.push_back(reinterpret_cast<uintptr_t>(adjoint_source[c]));
+    }
+    for (float v : p->src_vals) {
+        uint32_t b;
+        memcpy(&b, &v, 4);
+        key.push_back(b);
+    }
+    rc = p->opt.graph && !p->profiling
+             ? run_graph(p, p->gmis, key, st,
+                         [&](cudaStream_t s) { return gradient_enqueue(p, ws, nullptr, param, grad, nullptr, s, &mf); })
+             : gradient_enqueue(p, ws, nullptr, param, grad, nullptr, st, &mf);
     if (rc) return rc;
     // the last group's states are in the store: a pyfwi_gradient may follow
     // without another forward only if there is one group and nothing was recomputed

@@ -92,14 +92,36 @@ class Plan:
         sv = np.ascontiguousarray(src_vals, np.float32).reshape(-1, 4)
         if traces is None:
             traces = torch.empty((5, self.nt_ext, self.ns * self.nr), dtype=torch.float32, device=self.device)
-        grad = torch.empty((3, self.nz, self.nx), dtype=torch.float32, device=self.device)
-        misfit = torch.zeros((), dtype=torch.float64, device=self.device)
+        graph = bool(self.opts.graph)
+        if graph:
+            # the captured graph bakes in pointers: run on buffers the plan
+            # keeps and copy in / out around the replay
+            bufs = self.__dict__.setdefault("_mis_bufs", {})
+
+            def keep(name, like):
+                b = bufs.get(name)
+                if b is None or b.shape != like.shape or b.dtype != like.dtype:
+                    b = bufs[name] = torch.empty_like(like, memory_format=torch.contiguous_format)
+                return b
+            obs_in = [None if o is None else keep(("obs", q), o).copy_(o) for q, o in enumerate(observed)]
+            adj_in = [None if a is None else keep(("adj", q), a) for q, a in enumerate(adjoint)]
+            grad = keep("grad", torch.empty((3, self.nz, self.nx), dtype=torch.float32, device=self.device))
+            misfit = keep("misfit", torch.empty((), dtype=torch.float64, device=self.device))
+        else:
+            obs_in, adj_in = observed, adjoint
+            grad = torch.empty((3, self.nz, self.nx), dtype=torch.float32, device=self.device)
+            misfit = torch.zeros((), dtype=torch.float64, device=self.device)
         N.check(self.lib.pyfwi_misfit_gradient(self.handle, self.ws, self.ws_bytes,
                                                sv.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(sv.shape[0]),
-                                               _ptr_array(observed), int(bool(mean_stress)), _ptr_array(adjoint),
+                                               _ptr_array(obs_in), int(bool(mean_stress)), _ptr_array(adj_in),
                                                int(param), _ptr(traces), _ptr(grad), _ptr(misfit),
                                                _stream(self.device)))
         self._keep = (observed, adjoint)
+        if graph:
+            for a, b in zip(adjoint, adj_in):
+                if a is not None:
+                    a.copy_(b)
+            return grad.clone(), misfit.clone(), traces
         return grad, misfit, traces
 
     def check_device(self):

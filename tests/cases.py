@@ -317,4 +317,4 @@ def timelapse(method):
     return case
 
 
-TL_METHODS = ["cc", "dd", "sim"]
+TL_METHODS = ["pa", "cc", "dd", "sim", "wa", "cj", "cd", "cu"]
