@@ -100,7 +100,8 @@ typedef struct pyfwi_geometry {
  *   J = 1/2 sum (trace - observed)^2 of the discrete forward step of this
  *   library (transposed step, the absorbing profiles held fixed), on the whole
  *   model grid with no mask; the residual planes are dJ/dtrace per raw trace.
- *   Needs PYFWI_CKPT_EXACT with FP32 snapshots. */
+ *   Needs PYFWI_CKPT_EXACT and no energy terms; with PYFWI_SNAP_BF16 the
+ *   transposed step reads S_{t+1} and S_t from the BF16 snapshots. */
 enum pyfwi_adjoint { PYFWI_ADJOINT_REFERENCE = 0, PYFWI_ADJOINT_EXACT = 1 };
 
 typedef struct pyfwi_options {

@@ -216,6 +216,36 @@ __device__ __forceinline__ float gbwd(const float *f, long long i, long long s, 
     return r;
 }
 
+// The same differences of a BF16 snapshot plane, each value widened to float.
+__device__ __forceinline__ float ldh(const __nv_bfloat16 *f, long long i)
+{
+    return __bfloat162float(__ushort_as_bfloat16(__ldg(reinterpret_cast<const unsigned short *>(f) + i)));
+}
+
+template <int R>
+__device__ __forceinline__ float gfwd(const __nv_bfloat16 *f, long long i, long long s, const float *c)
+{
+    float r = c[0] * (ldh(f, i + s) - ldh(f, i));
+    r = fmaf(c[1], ldh(f, i + 2 * s) - ldh(f, i - s), r);
+    if (R == 4) {
+        r = fmaf(c[2], ldh(f, i + 3 * s) - ldh(f, i - 2 * s), r);
+        r = fmaf(c[3], ldh(f, i + 4 * s) - ldh(f, i - 3 * s), r);
+    }
+    return r;
+}
+
+template <int R>
+__device__ __forceinline__ float gbwd(const __nv_bfloat16 *f, long long i, long long s, const float *c)
+{
+    float r = c[0] * (ldh(f, i) - ldh(f, i - s));
+    r = fmaf(c[1], ldh(f, i + s) - ldh(f, i - 2 * s), r);
+    if (R == 4) {
+        r = fmaf(c[2], ldh(f, i + 2 * s) - ldh(f, i - 3 * s), r);
+        r = fmaf(c[3], ldh(f, i + 3 * s) - ldh(f, i - 4 * s), r);
+    }
+    return r;
+}
+
 // ---------------------------------------------------------------------------
 // kernel arguments
 // ---------------------------------------------------------------------------
@@ -1008,6 +1038,9 @@ struct ExactArgs {
     long long in_stride, out_stride;
     const float *s1, *s0;   // forward states S_{t+1}, S_t, slot 0 (FP32)
     long long s1_stride, s0_stride;
+    // BF16 snapshots instead (kernel instance BF): S_{t+1} always, S_t when
+    // s0h is set (else S_t is the FP32 restart state s0)
+    const __nv_bfloat16 *s1h, *s0h;
     const float *mat;       // lam, mu, b, rho planes
     const float *dampx, *dampz;
     float *gacc;            // [slot][3][plane]: Glam, Gmu, Gb
@@ -1038,7 +1071,7 @@ struct ExactShape {
     static constexpr int FLOATS = 3 * PW * PH + 2 * QW * QH;
 };
 
-template <int R, int TZ>
+template <int R, int TZ, bool BF>
 __global__ void __launch_bounds__(NTHREADS) exact_adj_step(const __grid_constant__ ExactArgs a)
 {
     using S = ExactShape<R, TZ>;
@@ -1053,7 +1086,10 @@ __global__ void __launch_bounds__(NTHREADS) exact_adj_step(const __grid_constant
     const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TZ;
     const float *L1 = a.in + slot * a.in_stride;
     float *L0 = a.out + slot * a.out_stride;
-    const float *S1 = a.s1 + slot * a.s1_stride, *S0 = a.s0 + slot * a.s0_stride;
+    const float *S1 = BF ? nullptr : a.s1 + slot * a.s1_stride;
+    const float *S0 = (BF && a.s0h) ? nullptr : a.s0 + slot * a.s0_stride;
+    const __nv_bfloat16 *H1 = BF ? a.s1h + slot * a.s1_stride : nullptr;
+    const __nv_bfloat16 *H0 = (BF && a.s0h) ? a.s0h + slot * a.s0_stride : nullptr;
     float *G = a.gacc + slot * a.gacc_stride;
     const float dt = a.k.dt;
 
@@ -1117,11 +1153,28 @@ __global__ void __launch_bounds__(NTHREADS) exact_adj_step(const __grid_constant
         L0[TXZ * P + co] = axz - dfwd<R>(q1, iq, QW, a.k.cz) - dbwd<R>(q2, iq, 1, a.k.cx);
         if (!dom) continue;
         const long long pz = g.pitch;
-        const float dxp_vx = gfwd<R>(S1 + VX * P, co, 1, a.k.cx), dzm_vz = gbwd<R>(S1 + VZ * P, co, pz, a.k.cz);
-        const float dxm_vz = gbwd<R>(S1 + VZ * P, co, 1, a.k.cx), dzp_vx = gfwd<R>(S1 + VX * P, co, pz, a.k.cz);
-        float dxm_tx = gbwd<R>(S0 + TXX * P, co, 1, a.k.cx), dzm_txz = gbwd<R>(S0 + TXZ * P, co, pz, a.k.cz);
-        float dzp_tz = gfwd<R>(S0 + TZZ * P, co, pz, a.k.cz);
-        const float dxp_txz = gfwd<R>(S0 + TXZ * P, co, 1, a.k.cx);
+        // velocity differences of S_{t+1}, stress differences of S_t
+        auto vdiffs = [&](const auto *S, float &xp_vx, float &zm_vz, float &xm_vz, float &zp_vx) {
+            xp_vx = gfwd<R>(S + VX * P, co, 1, a.k.cx);
+            zm_vz = gbwd<R>(S + VZ * P, co, pz, a.k.cz);
+            xm_vz = gbwd<R>(S + VZ * P, co, 1, a.k.cx);
+            zp_vx = gfwd<R>(S + VX * P, co, pz, a.k.cz);
+        };
+        auto sdiffs = [&](const auto *S, float &xm_tx, float &zm_txz, float &zp_tz, float &xp_txz) {
+            xm_tx = gbwd<R>(S + TXX * P, co, 1, a.k.cx);
+            zm_txz = gbwd<R>(S + TXZ * P, co, pz, a.k.cz);
+            zp_tz = gfwd<R>(S + TZZ * P, co, pz, a.k.cz);
+            xp_txz = gfwd<R>(S + TXZ * P, co, 1, a.k.cx);
+        };
+        float dxp_vx, dzm_vz, dxm_vz, dzp_vx, dxm_tx, dzm_txz, dzp_tz, dxp_txz;
+        if (BF)
+            vdiffs(H1, dxp_vx, dzm_vz, dxm_vz, dzp_vx);
+        else
+            vdiffs(S1, dxp_vx, dzm_vz, dxm_vz, dzp_vx);
+        if (H0)
+            sdiffs(H0, dxm_tx, dzm_txz, dzp_tz, dxp_txz);
+        else
+            sdiffs(S0, dxm_tx, dzm_txz, dzp_tz, dxp_txz);
         if (si == i) dxm_tx = fmaf(coef_bwd<R>(sj - j, a.k.cx), a.src.z, dxm_tx);  // S_t + source
         if (sj == j) dzp_tz = fmaf(coef_fwd<R>(si - i, a.k.cz), a.src.w, dzp_tz);
         G[0 * P + co] += dt * (axx + azz) * (dxp_vx + dzm_vz);
