@@ -473,31 +473,34 @@ def configs_run(args, dev):
     """The two smaller configurations (cases.c1: 100 x 100 cells, 4 shots,
     nt 500; cases.c2: 200 x 400 cells, 10 shots, nt 2000): one misfit and
     gradient evaluation of all shots on the device (CUDA events, 3 timed
-    after 1 untimed), and the reference's kernels on the host cores on one
-    shot (bounded sample, as cpu_baseline); Gcell-updates/s and shots/s."""
+    after 1 untimed; direct launches, and the plan replaying its captured
+    graph), and the reference's kernels on the host cores on one shot
+    (bounded sample, as cpu_baseline); Gcell-updates/s and shots/s."""
     import cases
     import torch
     from helpers import product
     out = {}
     for name in ("c1", "c2"):
         case = cases.by_name(name)
-        W = product(case, cuda_device=str(dev))
-        obs = {k: v.clone() for k, v in W.forward_modeling(
-            {k: torch.from_numpy(v).to(dev) for k, v in case["model_obs"].items()}).items()}
-        model = {k: torch.from_numpy(v).to(dev) for k, v in case["model_est"].items()}
-        per_shot = 2.0 * int(W.tnz) * int(W.tnx) * int(W.nt)
-        W.misfit_gradient(model, obs)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(3):
+        gpu = {}
+        for form, extra in (("launches", {}), ("graph", {"graph": True})):
+            W = product(case, cuda_device=str(dev), **extra)
+            obs = {k: v.clone() for k, v in W.forward_modeling(
+                {k: torch.from_numpy(v).to(dev) for k, v in case["model_obs"].items()}).items()}
+            model = {k: torch.from_numpy(v).to(dev) for k, v in case["model_est"].items()}
+            per_shot = 2.0 * int(W.tnz) * int(W.tnx) * int(W.nt)
             W.misfit_gradient(model, obs)
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / 3
-        gpu = {"ms_per_evaluation": ms, "value": per_shot * int(W.ns) / (ms * 1e-3) / 1e9, "unit": UNIT,
-               "shots_per_s": int(W.ns) / (ms * 1e-3)}
-        del W, obs
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(3):
+                W.misfit_gradient(model, obs)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / 3
+            gpu[form] = {"ms_per_evaluation": ms, "value": per_shot * int(W.ns) / (ms * 1e-3) / 1e9, "unit": UNIT,
+                         "shots_per_s": int(W.ns) / (ms * 1e-3)}
+            del W, obs
         cpu = None
         if not args.no_cpu:
             v, kind, cores, desc = cpu_sample(case, seconds=args.cpu_seconds / 3)

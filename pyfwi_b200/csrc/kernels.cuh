@@ -216,32 +216,35 @@ __device__ __forceinline__ float gbwd(const float *f, long long i, long long s, 
     return r;
 }
 
-// The same differences of a BF16 snapshot plane, each value widened to float.
+// The same differences with the values taken through a loader ld(index):
+// a BF16 snapshot plane widened to float, or an FP32 plane rounded to BF16
+// first (so that every forward state the BF16 exact adjoint reads carries
+// the same rounding, whichever slot holds it).
 __device__ __forceinline__ float ldh(const __nv_bfloat16 *f, long long i)
 {
     return __bfloat162float(__ushort_as_bfloat16(__ldg(reinterpret_cast<const unsigned short *>(f) + i)));
 }
 
-template <int R>
-__device__ __forceinline__ float gfwd(const __nv_bfloat16 *f, long long i, long long s, const float *c)
+template <int R, typename L>
+__device__ __forceinline__ float lfwd(L ld, long long i, long long s, const float *c)
 {
-    float r = c[0] * (ldh(f, i + s) - ldh(f, i));
-    r = fmaf(c[1], ldh(f, i + 2 * s) - ldh(f, i - s), r);
+    float r = c[0] * (ld(i + s) - ld(i));
+    r = fmaf(c[1], ld(i + 2 * s) - ld(i - s), r);
     if (R == 4) {
-        r = fmaf(c[2], ldh(f, i + 3 * s) - ldh(f, i - 2 * s), r);
-        r = fmaf(c[3], ldh(f, i + 4 * s) - ldh(f, i - 3 * s), r);
+        r = fmaf(c[2], ld(i + 3 * s) - ld(i - 2 * s), r);
+        r = fmaf(c[3], ld(i + 4 * s) - ld(i - 3 * s), r);
     }
     return r;
 }
 
-template <int R>
-__device__ __forceinline__ float gbwd(const __nv_bfloat16 *f, long long i, long long s, const float *c)
+template <int R, typename L>
+__device__ __forceinline__ float lbwd(L ld, long long i, long long s, const float *c)
 {
-    float r = c[0] * (ldh(f, i) - ldh(f, i - s));
-    r = fmaf(c[1], ldh(f, i + s) - ldh(f, i - 2 * s), r);
+    float r = c[0] * (ld(i) - ld(i - s));
+    r = fmaf(c[1], ld(i + s) - ld(i - 2 * s), r);
     if (R == 4) {
-        r = fmaf(c[2], ldh(f, i + 2 * s) - ldh(f, i - 3 * s), r);
-        r = fmaf(c[3], ldh(f, i + 3 * s) - ldh(f, i - 4 * s), r);
+        r = fmaf(c[2], ld(i + 2 * s) - ld(i - 3 * s), r);
+        r = fmaf(c[3], ld(i + 3 * s) - ld(i - 4 * s), r);
     }
     return r;
 }
@@ -1039,7 +1042,8 @@ struct ExactArgs {
     const float *s1, *s0;   // forward states S_{t+1}, S_t, slot 0 (FP32)
     long long s1_stride, s0_stride;
     // BF16 snapshots instead (kernel instance BF): S_{t+1} always, S_t when
-    // s0h is set (else S_t is the FP32 restart state s0)
+    // s0h is set (else S_t is the FP32 restart state s0, rounded to BF16 as
+    // it is read)
     const __nv_bfloat16 *s1h, *s0h;
     const float *mat;       // lam, mu, b, rho planes
     const float *dampx, *dampz;
@@ -1153,28 +1157,42 @@ __global__ void __launch_bounds__(NTHREADS) exact_adj_step(const __grid_constant
         L0[TXZ * P + co] = axz - dfwd<R>(q1, iq, QW, a.k.cz) - dbwd<R>(q2, iq, 1, a.k.cx);
         if (!dom) continue;
         const long long pz = g.pitch;
-        // velocity differences of S_{t+1}, stress differences of S_t
-        auto vdiffs = [&](const auto *S, float &xp_vx, float &zm_vz, float &xm_vz, float &zp_vx) {
-            xp_vx = gfwd<R>(S + VX * P, co, 1, a.k.cx);
-            zm_vz = gbwd<R>(S + VZ * P, co, pz, a.k.cz);
-            xm_vz = gbwd<R>(S + VZ * P, co, 1, a.k.cx);
-            zp_vx = gfwd<R>(S + VX * P, co, pz, a.k.cz);
+        // velocity differences of S_{t+1}, stress differences of S_t; ld(f)
+        // gives the loader of field f's plane
+        auto vdiffs = [&](auto ld, float &xp_vx, float &zm_vz, float &xm_vz, float &zp_vx) {
+            xp_vx = lfwd<R>(ld(VX), co, 1, a.k.cx);
+            zm_vz = lbwd<R>(ld(VZ), co, pz, a.k.cz);
+            xm_vz = lbwd<R>(ld(VZ), co, 1, a.k.cx);
+            zp_vx = lfwd<R>(ld(VX), co, pz, a.k.cz);
         };
-        auto sdiffs = [&](const auto *S, float &xm_tx, float &zm_txz, float &zp_tz, float &xp_txz) {
-            xm_tx = gbwd<R>(S + TXX * P, co, 1, a.k.cx);
-            zm_txz = gbwd<R>(S + TXZ * P, co, pz, a.k.cz);
-            zp_tz = gfwd<R>(S + TZZ * P, co, pz, a.k.cz);
-            xp_txz = gfwd<R>(S + TXZ * P, co, 1, a.k.cx);
+        auto sdiffs = [&](auto ld, float &xm_tx, float &zm_txz, float &zp_tz, float &xp_txz) {
+            xm_tx = lbwd<R>(ld(TXX), co, 1, a.k.cx);
+            zm_txz = lbwd<R>(ld(TXZ), co, pz, a.k.cz);
+            zp_tz = lfwd<R>(ld(TZZ), co, pz, a.k.cz);
+            xp_txz = lfwd<R>(ld(TXZ), co, 1, a.k.cx);
+        };
+        auto f32 = [&](const float *S) {
+            return [=](int f) { return [=](long long i) { return __ldg(S + f * P + i); }; };
+        };
+        auto b16 = [&](const __nv_bfloat16 *S) {
+            return [=](int f) { return [=](long long i) { return ldh(S + f * P, i); }; };
+        };
+        auto f32_as_b16 = [&](const float *S) {
+            return [=](int f) {
+                return [=](long long i) { return __bfloat162float(__float2bfloat16_rn(__ldg(S + f * P + i))); };
+            };
         };
         float dxp_vx, dzm_vz, dxm_vz, dzp_vx, dxm_tx, dzm_txz, dzp_tz, dxp_txz;
-        if (BF)
-            vdiffs(H1, dxp_vx, dzm_vz, dxm_vz, dzp_vx);
-        else
-            vdiffs(S1, dxp_vx, dzm_vz, dxm_vz, dzp_vx);
-        if (H0)
-            sdiffs(H0, dxm_tx, dzm_txz, dzp_tz, dxp_txz);
-        else
-            sdiffs(S0, dxm_tx, dzm_txz, dzp_tz, dxp_txz);
+        if (BF) {
+            vdiffs(b16(H1), dxp_vx, dzm_vz, dxm_vz, dzp_vx);
+            if (H0)
+                sdiffs(b16(H0), dxm_tx, dzm_txz, dzp_tz, dxp_txz);
+            else
+                sdiffs(f32_as_b16(S0), dxm_tx, dzm_txz, dzp_tz, dxp_txz);
+        } else {
+            vdiffs(f32(S1), dxp_vx, dzm_vz, dxm_vz, dzp_vx);
+            sdiffs(f32(S0), dxm_tx, dzm_txz, dzp_tz, dxp_txz);
+        }
         if (si == i) dxm_tx = fmaf(coef_bwd<R>(sj - j, a.k.cx), a.src.z, dxm_tx);  // S_t + source
         if (sj == j) dzp_tz = fmaf(coef_fwd<R>(si - i, a.k.cz), a.src.w, dzp_tz);
         G[0 * P + co] += dt * (axx + azz) * (dxp_vx + dzm_vz);

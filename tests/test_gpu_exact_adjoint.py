@@ -58,10 +58,11 @@ def test_exact_gradient_matches_fp64_oracle(name):
 @pytest.mark.parametrize("name", ["tiny_dxr", "tiny_dtscale"])
 def test_exact_adjoint_with_bf16_snapshots(name):
     """The exact adjoint reading BF16 snapshots (FP32 arithmetic; S_{t+1}
-    and S_t rounded to 8 mantissa bits, restart states FP32): the same
-    gradient bits for any recompute segment (the snapshots come from the same
-    FP32 chain), float32 rounding for another shot grouping, and within
-    1e-2 of the FP64 oracle's exact gradient."""
+    and S_t rounded to 8 mantissa bits, a segment's FP32 restart state
+    rounded the same way as it is read): the same gradient bits for any
+    recompute segment (the snapshots come from the same FP32 chain), float32
+    rounding for another shot grouping, and within 1e-2 of the FP64 oracle's
+    exact gradient."""
     import torch
     case = cases.by_name(name)
     d_obs = product(case).forward_modeling(case["model_obs"])
