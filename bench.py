@@ -423,7 +423,7 @@ def uneven_run(args, dev):
     from helpers import product
     from pyfwi_b200.batch import SurveyBatch
     cs = cases.c4(args.uneven)
-    props = [product(c, cuda_device=str(dev)) for c in cs]
+    props = [product(c, cuda_device=str(dev), graph=False) for c in cs]
     batch = SurveyBatch(props)  # shares the device memory out before any plan is built
     models, observed = [], []
     for W, c in zip(props, cs):
@@ -483,7 +483,7 @@ def configs_run(args, dev):
     for name in ("c1", "c2"):
         case = cases.by_name(name)
         gpu = {}
-        for form, extra in (("launches", {}), ("graph", {"graph": True})):
+        for form, extra in (("launches", {"graph": False}), ("graph", {"graph": True})):
             W = product(case, cuda_device=str(dev), **extra)
             obs = {k: v.clone() for k, v in W.forward_modeling(
                 {k: torch.from_numpy(v).to(dev) for k, v in case["model_obs"].items()}).items()}
@@ -512,12 +512,13 @@ def configs_run(args, dev):
 
 def plain_form(args, dev, batched_shots_s):
     """The plain form on the same survey: one shot per launch sequence
-    (shot_batch 1) with every forward step stored in FP32 (segment = nt), on
-    the first `--plain-shots` shots.  One untimed evaluation, one timed."""
+    (shot_batch 1) with every forward step stored in FP32 (segment = nt),
+    each launch issued from the host (no graph replay), on the first
+    `--plain-shots` shots.  One untimed evaluation, one timed."""
     import torch
     from helpers import product
     case = survey(args.plain_shots, args.nt)
-    extra = {"cuda_device": str(dev), "segment": 0, "shot_batch": 1}
+    extra = {"cuda_device": str(dev), "segment": 0, "shot_batch": 1, "graph": False}
     if args.tile is not None:
         extra["tile"] = args.tile if args.tile == "auto" else int(args.tile)
     if args.adj_tile is not None:

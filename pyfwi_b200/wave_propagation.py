@@ -16,7 +16,10 @@ default: 'exact' when chpr == 100, else the reference's reverse-time scheme),
 kernel variant, 0..5, or 'auto' to time them all on this survey first and
 take the fastest forward and adjoint variant), ``adj_tile`` (adjoint step
 variant when it differs from ``tile``), ``chunk`` (rows per CTA of the
-streaming variants), ``graph`` (replay whole calls as CUDA graphs),
+streaming variants), ``graph`` (replay whole calls as CUDA graphs: True,
+False, or 'auto', the default: on where a launch carries at most 8 M
+cell-shots, where issuing launches from the host would cost a noticeable
+share),
 ``snapshot`` ('fp32', or 'bf16': the forward states the imaging reads are
 stored in BF16 while the forward recurrence stays FP32; halves their memory
 and their reads at the cost of rounding the imaged fields to 8 bits),
@@ -276,7 +279,7 @@ class WavePreparation:
             o.energy = 1 if self.energy_balancing and self.adjoint != "exact" else 0
             o.tile, o.adj_tile = variants
             o.adjoint = N.ADJOINT_EXACT if self.adjoint == "exact" else N.ADJOINT_REFERENCE
-            o.graph = int(bool(inpa.get("graph", False)))
+            o.graph = int(self._graph_on(inpa.get("graph", "auto"), batch))
             o.chunk = int(inpa.get("chunk", 0))
             if chp is not None:
                 o.nchp = int(chp.size)
@@ -307,6 +310,22 @@ class WavePreparation:
         self._plan = Plan(geom, srcx, srcz, opts(seg, batch), self.device, chp=chp)
         self.segment, self.shot_batch = seg, batch
         self._tile, self._adj_tile = variants[0], (variants[1] - 1 if variants[1] else variants[0])
+
+    # 'auto' replays captured graphs where a launch carries at most this many
+    # cell-shots: there a step kernel runs for tens of microseconds or less and
+    # issuing it from the host costs a noticeable share (measured on B200:
+    # 100 x 100 + 20-cell layer, 4 shots: 1.9x; 200 x 400 + 20, 10 shots:
+    # 1.08x); above it the kernels hide the issue cost and the copies into
+    # the captured buffers are pure overhead
+    GRAPH_AUTO_CELLS = 8_000_000
+
+    def _graph_on(self, graph, batch):
+        if graph == "auto":
+            b = int(batch) if batch else int(self.ns)
+            return int(self.tnz) * int(self.tnx) * b <= self.GRAPH_AUTO_CELLS
+        if graph not in (True, False, 0, 1):
+            raise ValueError("inpa['graph'] must be True, False or 'auto'")
+        return bool(graph)
 
     # Layout cost model, in units of one forward step of one cell of one shot:
     # an adjoint+imaging step costs about 1.9 of them; a forward step has a
