@@ -236,6 +236,22 @@ int pyfwi_launch_count(const pyfwi_plan *plan, int64_t *count);
  * waits and no counterpart. */
 int pyfwi_device_error(pyfwi_plan *plan, void *workspace, size_t bytes, int32_t *code, void *stream);
 
+/* Memory check (the GPU pool has no sanitizer): count the nonzero cells of
+ * the zero frame around every FP32 plane of the workspace (materials, work
+ * and adjoint states, gradient accumulators, checkpoint store) after the work
+ * queued on `stream` (synchronises it).  The stencils read that frame as zero
+ * and no kernel writes it, so *nonzero != 0 means a write outside the update
+ * domain.  No reference counterpart. */
+int pyfwi_frame_check(pyfwi_plan *plan, void *workspace, size_t bytes, int64_t *nonzero, void *stream);
+
+/* Failure-path self test: one CTA waits on an mbarrier nothing arrives at,
+ * with the streaming kernels' bounded wait cut to `limit_ns` (1e3 .. 1e10) of
+ * the GPU's global timer, then gives up as they do and sets the workspace's
+ * error word to 1.  Until pyfwi_device_error reads and clears the word, the
+ * streaming kernels of later calls stop at once; the tile kernels run.  No
+ * reference counterpart. */
+int pyfwi_wait_selftest(pyfwi_plan *plan, void *workspace, size_t bytes, int64_t limit_ns, void *stream);
+
 /* Gradient evaluation that allocates no device memory.  No counterpart in
  * the reference (PyFWI allocates its buffers through pyopencl per
  * WavePropagator).  For callers that cannot call cudaMalloc -- e.g. a host

@@ -71,6 +71,8 @@ def lib():
     L.pyfwi_tile_count.argtypes = [_i32]
     L.pyfwi_launch_count.argtypes = [_P, ctypes.POINTER(ctypes.c_int64)]
     L.pyfwi_device_error.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(_i32), _P]
+    L.pyfwi_wait_selftest.argtypes = [_P, _P, ctypes.c_size_t, ctypes.c_int64, _P]
+    L.pyfwi_frame_check.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int64), _P]
     L.pyfwi_profile_enable.argtypes = [_P, _i32]
     L.pyfwi_profile_read.argtypes = [_P, _i32, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(ctypes.c_double)]
@@ -82,7 +84,8 @@ def lib():
     for name in ("pyfwi_plan_create", "pyfwi_plan_destroy", "pyfwi_workspace_size", "pyfwi_set_model",
                  "pyfwi_forward", "pyfwi_gradient", "pyfwi_l2_residual", "pyfwi_mean2", "pyfwi_tile_count",
                  "pyfwi_launch_count", "pyfwi_profile_enable", "pyfwi_profile_read", "pyfwi_device_error",
-                 "pyfwi_smooth", "pyfwi_misfit_gradient", "pyfwi_lowpass"):
+                 "pyfwi_smooth", "pyfwi_misfit_gradient", "pyfwi_lowpass", "pyfwi_wait_selftest",
+                 "pyfwi_frame_check"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

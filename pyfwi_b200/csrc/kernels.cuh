@@ -249,6 +249,23 @@ __device__ __forceinline__ float lbwd(L ld, long long i, long long s, const floa
     return r;
 }
 
+// Count the nonzero cells of the zero frame (rows outside [ZO, ZO + tnz),
+// columns outside [XO, XO + tnx)) of n consecutive planes: the stencils rely
+// on that frame reading as zero, and no kernel may write there.  NaN counts.
+__global__ void frame_check_kernel(const float *base, long long nplanes, Grid g, unsigned long long *count)
+{
+    unsigned long long local = 0;
+    const long long total = nplanes * g.plane;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long c = e % g.plane;
+        const int i = (int)(c / g.pitch), j = (int)(c - (long long)i * g.pitch);
+        const bool frame = i < ZO || i >= ZO + g.tnz || j < XO || j >= XO + g.tnx;
+        if (frame && !(base[e] == 0.f)) ++local;
+    }
+    if (local) atomicAdd(count, local);
+}
+
 // ---------------------------------------------------------------------------
 // kernel arguments
 // ---------------------------------------------------------------------------

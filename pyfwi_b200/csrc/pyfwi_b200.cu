@@ -9,6 +9,8 @@
 #include "kernels.cuh"
 #include "stream_kernels.cuh"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
@@ -19,6 +21,16 @@
 using namespace pyfwi;
 
 namespace {
+
+// NVTX range over a scope: the phases of a call show as named ranges in a
+// profiler's timeline (no cost without a profiler attached).
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range &) = delete;
+    Range &operator=(const Range &) = delete;
+};
+
 
 thread_local std::string g_err;
 
@@ -55,6 +67,7 @@ constexpr int STREAM_W[] = {0, 0, 0, 128, 64, 256};
 constexpr int N_TILES = 6;
 constexpr int FWD_PF = 4, ADJ_PF = 2;  // rows the streaming kernels fetch ahead
 constexpr size_t ERR_OFF = 128;         // byte offset of the device error word in the header
+constexpr size_t CHECK_OFF = 192;       // byte offset of the frame-check counter (uint64) in the header
 
 // cuTensorMapEncodeTiled, resolved through the runtime so the library does
 // not link the driver API directly
@@ -723,6 +736,7 @@ int gradient_enqueue(pyfwi_plan *p, void *ws, const float *const *residual, int3
     AdjArgs a = base_adj(p, ws, residual);
 
     for (int grp = 0; grp < p->ngroups; ++grp) {
+        Range range("pyfwi shot group: forward, residual, adjoint");
         int s0 = grp * p->G, n = std::min(p->G, G.ns - s0);
         a.shot0 = s0;
         if (mf) {  // model this group, then its residual
@@ -747,6 +761,7 @@ int gradient_enqueue(pyfwi_plan *p, void *ws, const float *const *residual, int3
             for (int m = p->M - 1; m >= 0; --m) {
                 int t_lo = m * p->seg, t_hi = std::min((m + 1) * p->seg, G.nt);
                 if (m < p->M - 1) {  // recompute segment m from its restart state
+                    Range range("pyfwi recompute segment");
                     for (int t = t_lo; t < t_hi; ++t) {
                         Buf in = exact_state(p, ws, t), out;
                         if (bf16_snaps(p)) {
@@ -773,6 +788,7 @@ int gradient_enqueue(pyfwi_plan *p, void *ws, const float *const *residual, int3
                         if (rc) return rc;
                     }
                 }
+                Range range("pyfwi adjoint segment");
                 for (int t = t_hi - 1; t >= std::max(t_lo, 1); --t) {
                     // forward state after step t: S_{t+1}
                     if (bf16_snaps(p)) {
@@ -871,6 +887,7 @@ int forward_enqueue(pyfwi_plan *p, void *ws, float *traces, cudaStream_t st)
     if (traces)
         CK(cudaMemsetAsync(traces, 0, 5 * (size_t)p->geom.nt_ext * p->geom.ns * p->geom.nr * sizeof(float), st));
     for (int grp = 0; grp < p->ngroups; ++grp) {
+        Range range("pyfwi shot group: forward");
         int s0 = grp * p->G, n = std::min(p->G, p->geom.ns - s0);
         int rc = p->opt.checkpoint == PYFWI_CKPT_EXACT ? exact_pass(p, ws, s0, n, traces, st)
                                                          : reverse_pass(p, ws, s0, n, traces, st);
@@ -1139,6 +1156,47 @@ int pyfwi_device_error(pyfwi_plan *p, void *ws, size_t bytes, int32_t *code, voi
     CK(cudaStreamSynchronize(st));
     *code = v;
     if (v) return fail(PYFWI_E_TIMEOUT, "device error word %d: a streaming kernel stopped early", v);
+    return PYFWI_OK;
+}
+
+int pyfwi_frame_check(pyfwi_plan *p, void *ws, size_t bytes, int64_t *nonzero, void *stream)
+{
+    if (!p || !nonzero) return fail(PYFWI_E_INVALID, "NULL argument");
+    int rc = check_ws(p, ws, bytes);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    auto *cnt = at<unsigned long long>(ws, CHECK_OFF);
+    CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st));
+    const long long G5 = 5LL * p->G;
+    long long store_planes = p->opt.checkpoint == PYFWI_CKPT_EXACT
+                                 ? store_stride(p) / p->g.plane * p->G
+                                 : (long long)p->chp.size() * 5 * p->geom.ns;
+    const struct {
+        size_t off;
+        long long planes;
+    } regions[] = {{p->o_mat, 4}, {p->o_work, 2 * G5}, {p->o_adj, 2 * G5}, {p->o_gacc, (long long)p->nacc * p->G},
+                   {p->o_store, store_planes}};
+    for (const auto &r : regions) {
+        if (r.planes <= 0) continue;
+        frame_check_kernel<<<4 * 148, 256, 0, st>>>(at<float>(ws, r.off), r.planes, p->g, cnt);
+        CKL();
+    }
+    unsigned long long v = 0;
+    CK(cudaMemcpyAsync(&v, cnt, sizeof v, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    *nonzero = (int64_t)v;
+    return PYFWI_OK;
+}
+
+int pyfwi_wait_selftest(pyfwi_plan *p, void *ws, size_t bytes, int64_t limit_ns, void *stream)
+{
+    if (!p) return fail(PYFWI_E_INVALID, "NULL plan");
+    if (limit_ns < 1000 || limit_ns > 10000000000LL) return fail(PYFWI_E_INVALID, "limit_ns outside [1e3, 1e10]");
+    int rc = check_ws(p, ws, bytes);
+    if (rc) return rc;
+    wait_selftest_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(at<int>(ws, ERR_OFF),
+                                                                          (unsigned long long)limit_ns);
+    CKL();
     return PYFWI_OK;
 }
 

@@ -72,18 +72,37 @@ __device__ __forceinline__ unsigned long long global_ns()
     return t;
 }
 
-// Wait for phase `parity` of `bar`; false (and the error word set) if it
-// does not complete within WAIT_NS.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int *err)
+// Wait for phase `parity` of `bar`; false (and the error word set to 1) if
+// it does not complete within `limit_ns` of the global timer.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t *bar, unsigned parity, int *err, unsigned long long limit_ns)
 {
     if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     while (!mbar_try(bar, parity))
-        if (global_ns() - t0 > WAIT_NS) {
+        if (global_ns() - t0 > limit_ns) {
             atomicExch(err, 1);
             return false;
         }
     return true;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int *err)
+{
+    return mbar_wait_for(bar, parity, err, WAIT_NS);
+}
+
+// The bounded wait on an mbarrier nothing arrives at: one thread waits
+// `limit_ns` and gives up as a streaming kernel does, so the timeout path
+// and the host's handling of the error word can be exercised on purpose.
+__global__ void wait_selftest_kernel(int *err, unsigned long long limit_ns)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) mbar_wait_for(&bar, 0, err, limit_ns);
 }
 
 // Tensor row of plane row r of the plane starting at p.

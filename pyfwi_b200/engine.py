@@ -131,6 +131,20 @@ class Plan:
         N.check(self.lib.pyfwi_device_error(self.handle, self.ws, self.ws_bytes, ctypes.byref(code),
                                             _stream(self.device)))
 
+    def frame_check(self):
+        """pyfwi_frame_check: nonzero cells in the zero frames of the
+        workspace planes (0 unless a kernel wrote outside its domain)."""
+        n = ctypes.c_int64()
+        N.check(self.lib.pyfwi_frame_check(self.handle, self.ws, self.ws_bytes, ctypes.byref(n),
+                                           _stream(self.device)))
+        return n.value
+
+    def wait_selftest(self, limit_ns):
+        """pyfwi_wait_selftest: a bounded device wait that nothing ends gives
+        up after limit_ns and sets the error word (read by check_device)."""
+        N.check(self.lib.pyfwi_wait_selftest(self.handle, self.ws, self.ws_bytes, int(limit_ns),
+                                             _stream(self.device)))
+
     def profile(self, enable=True):
         """Bracket every step kernel with CUDA events (see profile_read)."""
         N.check(self.lib.pyfwi_profile_enable(self.handle, 1 if enable else 0))
