@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PYFWI_ABI_VERSION 4
+#define PYFWI_ABI_VERSION 5
 
 enum pyfwi_status {
     PYFWI_OK = 0,
@@ -165,9 +165,16 @@ int pyfwi_forward(pyfwi_plan *plan, void *workspace, size_t workspace_bytes, con
 int pyfwi_gradient(pyfwi_plan *plan, void *workspace, size_t workspace_bytes, const float *const *residual,
                    int32_t parameterization, float *grad, float *raw, void *stream);
 
+/* Doubles of scratch a reduction needs (pyfwi_l2_residual): one partial sum
+ * per block of the reduction grid. */
+#define PYFWI_REDUCE_SLOTS 2368
+
 /* L2 misfit and residual (CostFunction.l2, fwi_tools.py:1402-1422):
- * res = est - obs (float32), *misfit += 0.5 * sum(res^2) (float64 sum on device). */
-int pyfwi_l2_residual(const float *est, const float *obs, float *res, int64_t n, double *misfit, void *stream);
+ * res = est - obs (float32), *misfit += 0.5 * sum(res^2) (float64 sum on
+ * device).  scratch: PYFWI_REDUCE_SLOTS device doubles for the per-block
+ * partial sums, added in a fixed order: the same inputs give the same bits. */
+int pyfwi_l2_residual(const float *est, const float *obs, float *res, int64_t n, double *scratch, double *misfit,
+                      void *stream);
 
 /* One misfit-and-gradient evaluation, the work of FWI.fprime (fwi.py:
  * 229-246: forward_modeling, CostFunction.l2 on the section, gradient) fused

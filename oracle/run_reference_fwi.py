@@ -62,8 +62,20 @@ def main():
 
     if "tl" in case:
         return _timelapse(case, inpa, src, shape, kw, d_obs, out_path)
+    s = case["fwi"]
+    m0 = {k: v.copy() for k, v in case["model_est"].items()}
+    param_functions = None
+    if "param_scale" in s:
+        # the model in units of `scale`: PyFWI's param_functions hooks
+        import PyFWI.fwi_tools as tools
+        scale = s["param_scale"]
+        param_functions = {"dict2vec": tools.vel_dict2vec, "vec2dict": tools.vec2vel_dict,
+                           "model_to_dv": lambda m, args: {k: v * args[0] for k, v in m.items()},
+                           "grad_from_dv": lambda g, args, m: {k: v * args[0] for k, v in g.items()},
+                           "args": [scale]}
+        m0 = {k: np.float32(v / np.float32(scale)) for k, v in m0.items()}
     F = fwi.FWI(d_obs, inpa, src, case["rec_loc"], shape, case["components"], case["chpr"],
-                n_well_rec=case.get("n_well_rec", 0))
+                n_well_rec=case.get("n_well_rec", 0), param_functions=param_functions)
     evals_m, evals_rms = [], []
     inner = F.fprime
 
@@ -73,9 +85,8 @@ def main():
         evals_rms.append(float(rms))
         return rms, grad
     F.fprime = recorded
-    s = case["fwi"]
-    m_est, rms = F({k: v.copy() for k, v in case["model_est"].items()}, s["method"], iter=s["iter"],
-                   freqs=s["freqs"], n_params=s["n_params"], k_0=s["k_0"], k_end=s["k_end"])
+    m_est, rms = F(m0, s["method"], iter=s["iter"], freqs=s["freqs"], n_params=s["n_params"], k_0=s["k_0"],
+                   k_end=s["k_end"])
     out = {"m_" + k: np.asarray(v, np.float64) for k, v in m_est.items()}
     out["evals_rms"] = np.asarray(evals_rms)
     out["evals_m"] = np.stack(evals_m)

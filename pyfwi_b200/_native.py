@@ -30,7 +30,8 @@ class Geometry(ctypes.Structure):
                 ("mask_row0", _i32), ("mask_row1", _i32), ("mask_col0", _i32), ("mask_col1", _i32)]
 
 
-ABI_VERSION = 4  # PYFWI_ABI_VERSION of include/pyfwi_b200.h
+ABI_VERSION = 5  # PYFWI_ABI_VERSION of include/pyfwi_b200.h
+REDUCE_SLOTS = 2368  # PYFWI_REDUCE_SLOTS
 
 
 class Options(ctypes.Structure):
@@ -62,7 +63,7 @@ def lib():
     L.pyfwi_set_model.argtypes = [_P, _P, ctypes.c_size_t, _P, _P, _P, _P, _P, _P]
     L.pyfwi_forward.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_float), _i32, _P, _P]
     L.pyfwi_gradient.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(_P), _i32, _P, _P, _P]
-    L.pyfwi_l2_residual.argtypes = [_P, _P, _P, ctypes.c_int64, _P, _P]
+    L.pyfwi_l2_residual.argtypes = [_P, _P, _P, ctypes.c_int64, _P, _P, _P]
     L.pyfwi_mean2.argtypes = [_P, _P, _P, ctypes.c_int64, _P]
     L.pyfwi_misfit_gradient.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_float), _i32,
                                         ctypes.POINTER(_P), _i32, ctypes.POINTER(_P), _i32, _P, _P, _P, _P]

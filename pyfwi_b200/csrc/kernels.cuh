@@ -1402,8 +1402,34 @@ __global__ void post_kernel(PostArgs a)
     }
 }
 
-// res = est - obs; misfit += 0.5 * sum(res^2)
-__global__ void l2_kernel(const float *est, const float *obs, float *res, long long n, double *misfit)
+// Sums that do not depend on scheduling: each block writes its partial sum
+// (a fixed tree over its threads) to partials[blockIdx.x]; one warp then adds
+// the partials in a fixed order.  Equal inputs give equal bits, so a line
+// search comparing two evaluations of the same model sees a tie as a tie.
+__device__ __forceinline__ void block_partial(double acc, double *partials)
+{
+    __shared__ double warp_sums[32];
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += warp_sums[w];
+        partials[blockIdx.x] = t;
+    }
+}
+
+// total += 0.5 * sum(partials[0..n)), one warp
+__global__ void sum_partials_kernel(const double *partials, int n, double *total)
+{
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < n; k += 32) acc += partials[k];
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (threadIdx.x == 0) *total += 0.5 * acc;
+}
+
+// res = est - obs; partials[block] = this block's share of sum(res^2)
+__global__ void l2_kernel(const float *est, const float *obs, float *res, long long n, double *partials)
 {
     double acc = 0.0;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
@@ -1411,8 +1437,7 @@ __global__ void l2_kernel(const float *est, const float *obs, float *res, long l
         res[k] = r;
         acc += (double)r * (double)r;
     }
-    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(misfit, 0.5 * acc);
+    block_partial(acc, partials);
 }
 
 // L2 misfit of one shot group's columns of the traces (CostFunction.l2,
@@ -1428,7 +1453,7 @@ struct MisfitArgs {
     float *res[5];
     long long nt, ncol, col0, ncols, plane;
     int mean_stress, exact;
-    double *misfit;
+    double *partials;      // one per block (block_partial)
 };
 
 __global__ void misfit_kernel(const MisfitArgs m)
@@ -1458,8 +1483,7 @@ __global__ void misfit_kernel(const MisfitArgs m)
             acc += (double)r * r;
         }
     }
-    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(m.misfit, 0.5 * acc);
+    block_partial(acc, m.partials);
 }
 
 __global__ void mean2_kernel(const float *a, const float *b, float *out, long long n)

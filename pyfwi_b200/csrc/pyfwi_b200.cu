@@ -93,7 +93,7 @@ struct pyfwi_plan {
     bool exact_adj = false;  // PYFWI_ADJOINT_EXACT
     long long state;  // floats per state (5 planes)
     // workspace offsets in bytes
-    size_t o_hdr, o_src, o_mat, o_dampx, o_dampz, o_work, o_adj, o_gacc, o_store, o_store16, total;
+    size_t o_hdr, o_src, o_red, o_mat, o_dampx, o_dampz, o_work, o_adj, o_gacc, o_store, o_store16, total;
     long long launches = 0;
     bool model_set = false, fwd_valid = false;
     // per-kernel event timing (pyfwi_profile_enable)
@@ -380,7 +380,7 @@ int step_adj(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s, const 
 int grid_blocks(long long n)
 {
     long long b = (n + 255) / 256;
-    return (int)(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
+    return (int)(b < PYFWI_REDUCE_SLOTS ? (b < 1 ? 1 : b) : PYFWI_REDUCE_SLOTS);
 }
 
 // ---- state addressing -------------------------------------------------------
@@ -695,6 +695,7 @@ struct Misfit {
     float *res[5];        // adjoint sources (written where used)
     int mean_stress;      // the stress keys hold (txx + tzz) / 2
     double *misfit;
+    double *partials;     // PYFWI_REDUCE_SLOTS block sums (workspace)
 };
 
 int misfit_group(pyfwi_plan *p, const Misfit &mf, int s0, int n, cudaStream_t st)
@@ -713,9 +714,12 @@ int misfit_group(pyfwi_plan *p, const Misfit &mf, int s0, int n, cudaStream_t st
     m.plane = (long long)G.nt_ext * G.ns * G.nr;
     m.mean_stress = mf.mean_stress;
     m.exact = p->exact_adj;
-    m.misfit = mf.misfit;
-    misfit_kernel<<<grid_blocks(m.nt * m.ncols), 256, 0, st>>>(m);
-    p->launches++;
+    m.partials = mf.partials;
+    const int nb = grid_blocks(m.nt * m.ncols);
+    misfit_kernel<<<nb, 256, 0, st>>>(m);
+    CKL();
+    sum_partials_kernel<<<1, 32, 0, st>>>(mf.partials, nb, mf.misfit);
+    p->launches += 2;
     CKL();
     return PYFWI_OK;
 }
@@ -1052,6 +1056,8 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
     o += ALIGN;
     p->o_src = o;
     o += up(2 * (size_t)G.ns * sizeof(int));
+    p->o_red = o;
+    o += up(PYFWI_REDUCE_SLOTS * sizeof(double));
     o = upr(o);
     p->o_mat = o;
     o += up(4 * pf);
@@ -1300,6 +1306,7 @@ int pyfwi_misfit_gradient(pyfwi_plan *p, void *ws, size_t bytes, const float *sr
     mf.traces = traces;
     mf.mean_stress = mean_stress != 0;
     mf.misfit = misfit;
+    mf.partials = at<double>(ws, p->o_red);
     bool any = false;
     for (int c = 0; c < 5; ++c) {
         mf.obs[c] = observed[c];
@@ -1335,11 +1342,16 @@ int pyfwi_misfit_gradient(pyfwi_plan *p, void *ws, size_t bytes, const float *sr
     return PYFWI_OK;
 }
 
-int pyfwi_l2_residual(const float *est, const float *obs, float *res, int64_t n, double *misfit, void *stream)
+int pyfwi_l2_residual(const float *est, const float *obs, float *res, int64_t n, double *scratch, double *misfit,
+                      void *stream)
 {
-    if (!est || !obs || !res || !misfit || n < 0) return fail(PYFWI_E_INVALID, "bad argument");
+    if (!est || !obs || !res || !scratch || !misfit || n < 0) return fail(PYFWI_E_INVALID, "bad argument");
     if (n == 0) return PYFWI_OK;
-    l2_kernel<<<grid_blocks(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(est, obs, res, n, misfit);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int nb = grid_blocks(n);
+    l2_kernel<<<nb, 256, 0, st>>>(est, obs, res, n, scratch);
+    CKL();
+    sum_partials_kernel<<<1, 32, 0, st>>>(scratch, nb, misfit);
     CKL();
     return PYFWI_OK;
 }

@@ -93,9 +93,11 @@ extern "C" int pyfwi_gradient_static(pyfwi_plan *plan, const float *vp, const fl
     const size_t comp = (size_t)nt_ext * ns * nr * sizeof(float);
     int n_obs = 0;
     for (int c = 0; c < 5; ++c) n_obs += observed[c] != nullptr;
-    // [workspace | traces (5 components) | residuals of the observed components]
+    // [workspace | traces (5 components) | residuals of the observed
+    // components | reduction scratch]
     const size_t o_traces = up256(ws_bytes), o_res = o_traces + up256(5 * comp);
-    const size_t need = o_res + (size_t)n_obs * up256(comp);
+    const size_t o_red = o_res + (size_t)n_obs * up256(comp);
+    const size_t need = o_red + up256(PYFWI_REDUCE_SLOTS * sizeof(double));
     if (need > (size_t)PYFWI_STATIC_SCRATCH_BYTES) {
         char msg[256];
         snprintf(msg, sizeof msg, "this survey needs %zu bytes of scratch; the library's static array holds %zu "
@@ -126,7 +128,9 @@ extern "C" int pyfwi_gradient_static(pyfwi_plan *plan, const float *vp, const fl
         if (!observed[c]) continue;
         float *r = reinterpret_cast<float *>(b + o_res + (size_t)q++ * up256(comp));
         const float *est = reinterpret_cast<const float *>(reinterpret_cast<const char *>(traces) + c * comp);
-        if ((rc = pyfwi_l2_residual(est, observed[c], r, (int64_t)nt_ext * ns * nr, misfit, stream))) return rc;
+        if ((rc = pyfwi_l2_residual(est, observed[c], r, (int64_t)nt_ext * ns * nr,
+                                    reinterpret_cast<double *>(b + o_red), misfit, stream)))
+            return rc;
         res[c] = r;
     }
     return pyfwi_gradient(plan, base, ws_bytes, res, parameterization, grad, nullptr, stream);

@@ -254,11 +254,13 @@ def l2_residual(dest, dobs):
     first = dest[[*dest][0]]
     dev = require_cuda(first.device)
     acc = torch.zeros((), dtype=torch.float64, device=dev)
+    scratch = torch.empty(N.REDUCE_SLOTS, dtype=torch.float64, device=dev)
     res = {}
     for p in dest:
         e = dest[p].to(dev, torch.float32).contiguous()
         o = dobs[p].to(dev, torch.float32).contiguous()
         r = torch.empty_like(e)
-        N.check(N.lib().pyfwi_l2_residual(_ptr(e), _ptr(o), _ptr(r), e.numel(), _ptr(acc), _stream(dev)))
+        N.check(N.lib().pyfwi_l2_residual(_ptr(e), _ptr(o), _ptr(r), e.numel(), _ptr(scratch), _ptr(acc),
+                                          _stream(dev)))
         res[p] = r
     return acc, res

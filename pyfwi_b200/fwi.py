@@ -3,11 +3,11 @@ propagator.
 
 Same constructor and ``__call__(m0, method, iter, freqs, n_params, k_0,
 k_end)``.  Each misfit evaluation runs forward modelling, the L2 residual
-and the adjoint gradient on the device.  ``lbfgs`` runs the reference's
-L-BFGS-B settings with the model, gradient and history vectors on the
-device (lbfgs.minimize); ``inpa['optimizer'] = 'scipy'`` hands the vectors
-to SciPy's ``fmin_l_bfgs_b`` on the host instead, as the reference does.
-``cg`` is SciPy's ``fmin_cg`` on the host.  The multiscale frequencies
+and the adjoint gradient on the device.  ``lbfgs`` and ``cg`` run the
+reference's L-BFGS-B and Polak-Ribiere+ settings with the model, gradient
+and history vectors on the device (lbfgs.minimize, cg.minimize);
+``inpa['optimizer'] = 'scipy'`` hands the vectors to SciPy's
+``fmin_l_bfgs_b`` / ``fmin_cg`` on the host instead, as the reference does.  The multiscale frequencies
 (`freqs`) low-pass the data on the device (fwi_tools.lowpass).
 Regularisation terms (TV, Tikhonov, prior, parameter relations) are not
 provided: asking for them raises."""
@@ -17,6 +17,7 @@ from scipy.optimize import fmin_cg, fmin_l_bfgs_b
 
 from . import acquisition as acq
 from . import fwi_tools as tools
+from . import cg as device_cg
 from . import lbfgs as device_lbfgs
 from .processing import COMPONENTS, prepare_residual
 from .wave_propagation import WavePropagator
@@ -150,6 +151,11 @@ class FWI(WavePropagator):
         raise ValueError("unknown optimisation method %r" % (user_method,))
 
     def cg(self, m0, ITER, freq, n_params=1, k0=1, k_end=2):
+        """Conjugate gradient over parameters k0, k0 + n_params, ... < k_end in
+        turn, ITER iterations each (fwi.py:162-195), the others held fixed."""
+        if self.optimizer == "device":
+            return self._device_run(device_cg.minimize, dict(gtol=1e-8, maxiter=ITER), m0, freq, n_params, k0,
+                                    k_end)
         n = self.nz * self.nx
         mtotal = np.copy(m0)
         hist = []
@@ -166,7 +172,8 @@ class FWI(WavePropagator):
         """L-BFGS over parameters k0, k0 + n_params, ... < k_end in turn, ITER
         iterations each (fwi.py:197-226), the others held fixed."""
         if self.optimizer == "device":
-            return self._lbfgs_device(m0, ITER, freq, n_params, k0, k_end)
+            return self._device_run(device_lbfgs.minimize, dict(m=10, factr=1e7, pgtol=1e-8, maxfun=15000,
+                                                                maxiter=ITER, maxls=10), m0, freq, n_params, k0, k_end)
         n = self.nz * self.nx
         mtotal = np.copy(m0)
         hist = []
@@ -180,14 +187,14 @@ class FWI(WavePropagator):
             mtotal = np.hstack((m_1, m_opt, m1))
         return mtotal, hist
 
-    def _lbfgs_device(self, m0, ITER, freq, n_params, k0, k_end):
+    def _device_run(self, minimize, settings, m0, freq, n_params, k0, k_end):
+        """The parameter loop of cg / lbfgs with the optimiser on the device."""
         n = self.nz * self.nx
         mtotal = torch.from_numpy(np.asarray(m0, np.float64)).to(self.device)
         hist = []
         for k in np.arange(k0, k_end, n_params):
             m_1, m_opt, m1 = mtotal[:k * n], mtotal[k * n:(k + n_params) * n], mtotal[(k + n_params) * n:]
-            res = device_lbfgs.minimize(lambda x: self.fprime_single(x, m_1, m1, freq), m_opt, m=10, factr=1e7,
-                                        pgtol=1e-8, maxfun=15000, maxiter=ITER, maxls=10)
+            res = minimize(lambda x: self.fprime_single(x, m_1, m1, freq), m_opt, **settings)
             hist.append(res.f)
             mtotal = torch.cat((m_1, res.x, m1))
         return mtotal.cpu().numpy(), hist

@@ -303,6 +303,20 @@ def fwi_lbfgs():
     return case
 
 
+def fwi_cg():
+    """fwi_lbfgs with the conjugate-gradient method, inverting for the model
+    in units of 2000 (m/s, kg/m^3) through PyFWI's param_functions (the
+    model passed in and returned scaled, model_to_dv multiplying by 2000,
+    grad_from_dv the gradient by 2000).  In physical units fmin_cg's first
+    trial step (at most 1) moves this model by less than its float32
+    rounding and the run takes no step; scaled, it moves a few m/s."""
+    case = fwi_lbfgs()
+    case["name"] = "fwi_cg"
+    case["fwi"]["method"] = "cg"
+    case["fwi"]["param_scale"] = 2000.0
+    return case
+
+
 def timelapse(method):
     """Time-lapse inversion on tiny_dxr: baseline = the case's observed
     model, monitor = baseline with vp -8 % in a 6 x 8-cell patch (a depleted

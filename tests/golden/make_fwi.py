@@ -1,4 +1,4 @@
-"""Regenerate tests/golden/fwi_lbfgs.npz and tests/golden/tl_<method>.npz
+"""Regenerate tests/golden/fwi_lbfgs.npz, fwi_cg.npz and tl_<method>.npz
 from the PyFWI reference.
 
     python tests/golden/make_fwi.py [name ...]
@@ -6,7 +6,7 @@ from the PyFWI reference.
 Runs the unmodified reference inversion drivers (``PyFWI.fwi.FWI`` and
 ``PyFWI.tl_fwi.TimeLapse`` with SciPy's L-BFGS-B, on PyFWI's own OpenCL C
 kernels compiled for the CPU, see oracle/run_reference_fwi.py) on the
-``fwi_lbfgs`` and ``timelapse(method)`` cases of tests/cases.py and stores
+``fwi_lbfgs``, ``fwi_cg`` and ``timelapse(method)`` cases of tests/cases.py and stores
 the resulting models and the misfit of every evaluation (for FWI also the
 model of every evaluation).  Needs the reference tree, so it runs only
 where that exists.
@@ -38,7 +38,7 @@ def make(case):
 
 
 def all_cases():
-    return [cases.fwi_lbfgs()] + [cases.timelapse(m) for m in cases.TL_METHODS]
+    return [cases.fwi_lbfgs(), cases.fwi_cg()] + [cases.timelapse(m) for m in cases.TL_METHODS]
 
 
 if __name__ == "__main__":

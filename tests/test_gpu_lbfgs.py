@@ -1,5 +1,5 @@
-"""FWI.lbfgs with the optimiser on the device (pyfwi_b200.lbfgs) on the
-two-stage inversion of cases.fwi_lbfgs (vp, vs, rho in turn, two L-BFGS
+"""FWI.lbfgs and FWI.cg with the optimiser on the device (pyfwi_b200.lbfgs,
+pyfwi_b200.cg) on the two-stage inversion of cases.fwi_lbfgs / fwi_cg (vp, vs, rho in turn, two L-BFGS
 iterations each, at 60 Hz and then full band: 12 iterations, ~30
 evaluations), against
 
@@ -31,6 +31,26 @@ pytestmark = pytest.mark.gpu
 KEYS = ("vp", "vs", "rho")
 
 
+def _param_functions(case):
+    """PyFWI param_functions for a case inverting in scaled units (as the
+    fixture's run did), or None."""
+    scale = case["fwi"].get("param_scale")
+    if scale is None:
+        return None
+    from pyfwi_b200 import fwi_tools as tools
+    return {"dict2vec": tools.vel_dict2vec, "vec2dict": tools.vec2vel_dict,
+            "model_to_dv": lambda m, args: {k: v * args[0] for k, v in m.items()},
+            "grad_from_dv": lambda g, args, m: {k: v * args[0] for k, v in g.items()}, "args": [scale]}
+
+
+def _start(case):
+    """The starting model as the driver receives it (scaled units if any)."""
+    scale = case["fwi"].get("param_scale")
+    if scale is None:
+        return {k: v.copy() for k, v in case["model_est"].items()}
+    return {k: np.float32(v / np.float32(scale)) for k, v in case["model_est"].items()}
+
+
 def _fwi(case, **extra):
     from pyfwi_b200 import acquisition as acq
     from pyfwi_b200.fwi import FWI
@@ -41,7 +61,7 @@ def _fwi(case, **extra):
     src = acq.Source(case["src_loc"], inpa["dh"], inpa["dt"], case["src_type"])
     src.Ricker(case["fdom"])
     return FWI(d_obs, inpa, src, case["rec_loc"], case["model_est"]["vp"].shape, components=case["components"],
-               chpr=case["chpr"], n_well_rec=case["n_well_rec"])
+               chpr=case["chpr"], n_well_rec=case["n_well_rec"], param_functions=_param_functions(case))
 
 
 def _run(case, **extra):
@@ -57,8 +77,8 @@ def _run(case, **extra):
         return rms, grad
     F.fprime = recorded
     s = case["fwi"]
-    m, _ = F({k: v.copy() for k, v in case["model_est"].items()}, s["method"], iter=s["iter"], freqs=s["freqs"],
-             n_params=s["n_params"], k_0=s["k_0"], k_end=s["k_end"])
+    m, _ = F(_start(case), s["method"], iter=s["iter"], freqs=s["freqs"], n_params=s["n_params"], k_0=s["k_0"],
+             k_end=s["k_end"])
     return m, evals
 
 
@@ -88,23 +108,28 @@ def _update_error(m, m_ref, m0):
     return rel_l2(upd, upd_ref)
 
 
-def test_device_lbfgs_matches_reference_inversion():
-    case = cases.fwi_lbfgs()
-    with np.load(GOLDEN + "/fwi_lbfgs.npz") as f:
+@pytest.mark.parametrize("name", ["fwi_lbfgs", "fwi_cg"])
+def test_device_optimiser_matches_reference_inversion(name):
+    """fwi_cg: the reference's fmin_cg takes no step on this case (the
+    Wolfe searches try steps below the float32 rounding of the model and give
+    up); the device CG must take the same 240 evaluations without moving."""
+    case = getattr(cases, name)()
+    with np.load(GOLDEN + "/%s.npz" % name) as f:
         ref = {k: f[k] for k in f.files}
     m, evals = _run(case)
-    m0 = np.concatenate([case["model_est"][k].reshape(-1).astype(np.float64) for k in KEYS])
+    m0 = np.concatenate([_start(case)[k].reshape(-1).astype(np.float64) for k in KEYS])
     _same_path(evals, list(zip(ref["evals_m"].astype(np.float64), ref["evals_rms"])), m0)
     err = _update_error(m, {k: ref["m_" + k] for k in KEYS}, m0)
     print("final model update vs reference: rel-L2 %.2e over %d evaluations" % (err, len(evals)))
     assert err <= UPDATE_TOL
 
 
-def test_device_lbfgs_matches_host_scipy_on_device_gradients():
+@pytest.mark.parametrize("name", ["fwi_lbfgs", "fwi_cg"])
+def test_device_optimiser_matches_host_scipy_on_device_gradients(name):
     """Same algorithm, same gradients: the two optimisers differ only in
     float64 rounding, so the first evaluations see the same float32 models
     bit for bit; later a cell's float32 rounding can flip."""
-    case = cases.fwi_lbfgs()
+    case = getattr(cases, name)()
     m_d, ev_d = _run(case)
     m_h, ev_h = _run(case, optimizer="scipy")
     m0 = ev_h[0][0]
