@@ -205,8 +205,11 @@ class FWI(WavePropagator):
         A device tensor m0 gives a device gradient."""
         if isinstance(m0, torch.Tensor) and not self._default_params:
             # user parameter functions work on numpy vectors, as in the reference
-            rms, grad = self.fprime(m0.cpu().numpy(), freq)
+            rms, grad = self._fprime(m0.cpu().numpy(), freq)
             return rms, torch.from_numpy(grad).to(m0.device)
+        return self._fprime(m0, freq)
+
+    def _fprime(self, m0, freq):
         m_old = self.vec2dict(m0.clone() if isinstance(m0, torch.Tensor) else np.copy(m0), self.nz, self.nx)
         m_new = self.model_to_dv(m_old, self.param_functions_args)
         model = {k: self._to_device(m_new[k]) for k in ("vp", "vs", "rho")}
