@@ -66,6 +66,23 @@ def test_end_to_end_gradient_within_tolerance(name):
         assert rel_l2(v, g["grad_" + k]) < GRAD_TOL, ("grad", k, rel_l2(v, g["grad_" + k]))
 
 
+@pytest.mark.parametrize("name", ["tiny_dxr", "tiny_both"])
+def test_three_d_section_shape(name):
+    """inpa['seimogram_shape'] = '3d': sections come as (nt, nr, ns), the
+    reference's array before its Fortran-order reshape to '2d'
+    (acquisition.py:313-333)."""
+    g = load_golden(name)
+    case = cases.by_name(name)
+    case["inpa"] = dict(case["inpa"], seimogram_shape="3d")
+    W = product(case)
+    d = W.forward_modeling(case["model_est"])
+    for k, v in d.items():
+        ref2 = g["d_est_" + k]
+        nt, nrs = ref2.shape
+        assert v.shape == (nt, int(W.nr), int(W.ns)), (k, v.shape)
+        assert rel_l2(np.reshape(v, (nt, nrs), order="F"), ref2) < SEIS_TOL, k
+
+
 @pytest.mark.parametrize("tile", VARIANTS + [1, 2])
 def test_fluid_keeps_normal_stresses_equal(tile):
     """In the water layer (mu = 0) the reference's txx and tzz stay the same
