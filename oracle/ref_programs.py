@@ -17,7 +17,7 @@ import cases  # noqa: E402
 import oracle as O  # noqa: E402
 import ref_build  # noqa: E402
 
-BASELINE_CASES = ["c1", "c2", "c3"]
+HOST_SAMPLE_CASES = ["c1", "c2", "c3"]
 
 
 def geometry_of(case):
@@ -35,7 +35,7 @@ def geometry_of(case):
                    rec_surface_const=int(W.rec_surface_const), rec_surface_var=int(W.rec_surface_var))
 
 
-def build_all(names=BASELINE_CASES):
+def build_all(names=HOST_SAMPLE_CASES):
     if not os.path.isdir(ref_build.REF_SRC):
         return {}
     out = {}
