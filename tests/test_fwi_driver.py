@@ -114,7 +114,8 @@ def test_user_parameter_functions_see_numpy_on_the_device_path():
     pf = {"dict2vec": tools.vel_dict2vec, "vec2dict": tools.vec2vel_dict, "model_to_dv": to_dv,
           "grad_from_dv": lambda g, args, m: {k: v * args[0] for k, v in g.items()}, "args": [2.0]}
     F, case = _fwi("device", param_functions=pf)
-    # misfit through the real fprime path up to model_to_dv: stop there
+    # stand in for the propagator part of fprime, which calls the user
+    # functions, to see what it is handed
     F._fprime = lambda m0, freq: (seen.append(type(m0)) or (0.0, np.zeros_like(np.asarray(m0, np.float64))))
     F.fprime(torch.zeros(3 * F.nz * F.nx, dtype=torch.float32), 0)
     assert seen and seen[0] is np.ndarray
