@@ -292,6 +292,49 @@ def c4(n_models=32, seed=44):
     return out
 
 
+def c5(ns=128, seed=55):
+    """The thrust-belt survey: 1000 x 3000 cells, dh = 4 m, 40-cell layer;
+    folded layers (vp 1500 -> 4500 m/s with depth, sinusoidal folds and two
+    thrust offsets), vs = vp / 1.75 except a 40-cell water layer (vp 1500,
+    vs 0, rho 1000), Gardner rho; ns explosive 6 Hz shots and 2000
+    receivers (every 1.5 cells) at 2 cells depth in the water; dt = 0.4 ms,
+    nt = 6000; pressure recorded.  The estimate is the model smoothed
+    (20-cell Gaussian, water kept); ``model_mon`` is the model with vp -8 %
+    in a 40 x 200-cell reservoir patch (the time-lapse monitor)."""
+    from scipy.ndimage import gaussian_filter
+    nz, nx, dh, dt = 1000, 3000, 4.0, 0.0004
+    rng = np.random.default_rng(seed)
+    z = np.arange(nz)[:, None].astype(np.float64)
+    x = np.arange(nx)[None, :].astype(np.float64)
+    fold = 60.0 * np.sin(2 * np.pi * x / rng.uniform(900, 1400)) * np.exp(-((z - 500) / 400) ** 2)
+    depth = z + fold + 80.0 * (x > rng.uniform(900, 1300)) + 60.0 * (x > rng.uniform(1900, 2300))
+    vp = 1800.0 + 2700.0 * np.clip((depth - 40) / (nz - 40), 0, 1)
+    vp = vp + 150.0 * np.sign(np.sin(depth / rng.uniform(60, 90)))
+    vp = np.clip(vp, 1500.0, 4500.0)
+    vp[:40] = 1500.0
+    vp = vp.astype(np.float32)
+    vs = (vp / 1.75).astype(np.float32)
+    vs[:40] = 0.0
+    rho = (310 * vp ** 0.25).astype(np.float32)
+    rho[:40] = 1000.0
+    model = {"vp": vp, "vs": vs, "rho": rho}
+    est = {"vp": gaussian_filter(vp, 20.0).astype(np.float32)}
+    est["vp"][:40] = 1500.0
+    est["vs"] = (est["vp"] / 1.75).astype(np.float32)
+    est["vs"][:40] = 0.0
+    est["rho"] = (310 * est["vp"] ** 0.25).astype(np.float32)
+    est["rho"][:40] = 1000.0
+    mon = {k: v.copy() for k, v in model.items()}
+    mon["vp"][600:640, 1400:1600] *= np.float32(0.92)
+    inpa = {"dt": dt, "t": _t_for(6000, dt), "dh": dh, "npml": 40, "pmlR": 1e-5, "pml_dir": 2, "sdo": 4,
+            "rec_dis": 1.5 * dh, "acq_type": 1}
+    src_loc = np.stack([np.linspace(40, nx - 41, ns).astype(np.int32) * dh, np.full(ns, 2 * dh)],
+                       1).astype(np.float32)
+    rec_loc = np.stack([np.arange(2000) * 1.5 * dh, np.full(2000, 2 * dh)], 1).astype(np.float32)
+    return dict(name="c5", inpa=inpa, src_loc=src_loc, rec_loc=rec_loc, fdom=6.0, src_type=0, components=0,
+                chpr=100, n_well_rec=0, param="dv", model_obs=model, model_est=est, model_mon=mon)
+
+
 def fwi_lbfgs():
     """The inversion driver on tiny_dxr: FWI(...)(m0, 'lbfgs', iter=[2, 2],
     freqs=[60, 0], n_params=1, k_0=1, k_end=4), i.e. vp, then vs, then rho,
