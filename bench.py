@@ -111,11 +111,16 @@ def dist_setup(args):
     return world, rank, local
 
 
-def survey(ns, nt=None):
-    """The 500 x 1000-cell survey with ns shots; nt < 4000 shortens the
-    record (small profiling cases only)."""
+THRUST_BELT = ("elastic FWI gradient, thrust-belt survey: 1000x3000 cells (+40-cell absorbing layer, 40-cell "
+               "water layer), %d of its 128 shots, 2000 receivers, nt=6000")
+
+
+def survey(ns, nt=None, config="c3"):
+    """The 500 x 1000-cell survey (config 'c3') or the 1000 x 3000 thrust-belt
+    survey ('c5') with ns shots; nt shortens the record (small profiling
+    cases only)."""
     import cases
-    case = cases.c3(ns=ns)
+    case = cases.c3(ns=ns) if config == "c3" else cases.c5(ns=ns)
     if nt:
         dt = case["inpa"]["dt"]
         case["inpa"]["t"] = (nt - 1) * dt + dt / 2
@@ -209,7 +214,7 @@ def run_ours(args, world, rank, local):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    case = survey(args.shots, args.nt)
+    case = survey(args.shots, args.nt, args.config)
     extra = {"cuda_device": str(dev)}
     if args.segment:
         extra.update(segment=args.segment, shot_batch=args.shots)
@@ -353,7 +358,8 @@ def run_ours(args, world, rank, local):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "shots_per_gpu": shape["ns"], "nt": shape["nt"],
+            "config": {"workload": WORKLOAD if args.config == "c3" else THRUST_BELT % shape["ns"],
+                       "shots_per_gpu": shape["ns"], "nt": shape["nt"],
                        "grid": shape["grid"], **layout, "parallelism": "dp%d" % world,
                        "l2": "inputs larger than L2 (no flush)"},
             "roofline": roof, "cpu_baseline": cpu, "plain": plain,
@@ -570,6 +576,8 @@ def main():
                     help="also time this many L-BFGS iterations of FWI (device and host optimiser)")
     ap.add_argument("--uneven", type=int, default=0,
                     help="also time a batch of this many uneven-size surveys (sequential, streams, graph)")
+    ap.add_argument("--config", choices=["c3", "c5"], default="c3",
+                    help="survey of the timed evaluation: the 500 x 1000 one (default) or the thrust-belt one")
     ap.add_argument("--configs", action="store_true",
                     help="also time the 100 x 100 and 200 x 400 configurations (device and host reference)")
     args = ap.parse_args()
