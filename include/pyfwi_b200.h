@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PYFWI_ABI_VERSION 5
+#define PYFWI_ABI_VERSION 6
 
 enum pyfwi_status {
     PYFWI_OK = 0,
@@ -242,6 +242,16 @@ int pyfwi_launch_count(const pyfwi_plan *plan, int64_t *count);
  * Returns PYFWI_E_TIMEOUT when *code != 0.  The reference has no device-side
  * waits and no counterpart. */
 int pyfwi_device_error(pyfwi_plan *plan, void *workspace, size_t bytes, int32_t *code, void *stream);
+
+/* The forward states a reverse-mode plan keeps at its checkpoint steps, the
+ * reference's WavePropagator.W (wave_propagation.py:150-156, filled at
+ * :710-727): for shot s, checkpoint k and field f (vx, vz, taux, tauz,
+ * tauxz), the state after internal step chp[k] on the padded grid.
+ *   out  device [ns][nchp][5][nz+2npml][nx+2npml]
+ * Valid after pyfwi_forward (pyfwi_gradient only reads the store).  Plans in
+ * exact mode keep no such store: PYFWI_E_STATE.  Device-to-device copies on
+ * `stream`; no kernel. */
+int pyfwi_checkpoint_states(pyfwi_plan *plan, void *workspace, size_t bytes, float *out, void *stream);
 
 /* Memory check (the GPU pool has no sanitizer): count the nonzero cells of
  * the zero frame around every FP32 plane of the workspace (materials, work

@@ -30,7 +30,7 @@ class Geometry(ctypes.Structure):
                 ("mask_row0", _i32), ("mask_row1", _i32), ("mask_col0", _i32), ("mask_col1", _i32)]
 
 
-ABI_VERSION = 5  # PYFWI_ABI_VERSION of include/pyfwi_b200.h
+ABI_VERSION = 6  # PYFWI_ABI_VERSION of include/pyfwi_b200.h
 REDUCE_SLOTS = 2368  # PYFWI_REDUCE_SLOTS
 
 
@@ -74,6 +74,7 @@ def lib():
     L.pyfwi_device_error.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(_i32), _P]
     L.pyfwi_wait_selftest.argtypes = [_P, _P, ctypes.c_size_t, ctypes.c_int64, _P]
     L.pyfwi_frame_check.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int64), _P]
+    L.pyfwi_checkpoint_states.argtypes = [_P, _P, ctypes.c_size_t, _P, _P]
     L.pyfwi_profile_enable.argtypes = [_P, _i32]
     L.pyfwi_profile_read.argtypes = [_P, _i32, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(ctypes.c_double)]
@@ -86,7 +87,7 @@ def lib():
                  "pyfwi_forward", "pyfwi_gradient", "pyfwi_l2_residual", "pyfwi_mean2", "pyfwi_tile_count",
                  "pyfwi_launch_count", "pyfwi_profile_enable", "pyfwi_profile_read", "pyfwi_device_error",
                  "pyfwi_smooth", "pyfwi_misfit_gradient", "pyfwi_lowpass", "pyfwi_wait_selftest",
-                 "pyfwi_frame_check"):
+                 "pyfwi_frame_check", "pyfwi_checkpoint_states"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

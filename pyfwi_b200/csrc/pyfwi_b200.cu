@@ -1165,6 +1165,27 @@ int pyfwi_device_error(pyfwi_plan *p, void *ws, size_t bytes, int32_t *code, voi
     return PYFWI_OK;
 }
 
+int pyfwi_checkpoint_states(pyfwi_plan *p, void *ws, size_t bytes, float *out, void *stream)
+{
+    if (!p || !out) return fail(PYFWI_E_INVALID, "NULL argument");
+    int rc = check_ws(p, ws, bytes);
+    if (rc) return rc;
+    if (p->opt.checkpoint != PYFWI_CKPT_REVERSE)
+        return fail(PYFWI_E_STATE, "only reverse-mode plans keep the checkpoint states");
+    if (!p->fwd_valid) return fail(PYFWI_E_STATE, "pyfwi_checkpoint_states needs a pyfwi_forward first");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const Grid &g = p->g;
+    // store: per shot, per checkpoint, one state of 5 planes (chp_state)
+    const long long nplanes = (long long)p->geom.ns * (long long)p->chp.size() * 5;
+    const float *store = at<float>(ws, p->o_store);
+    const long long cells = (long long)g.tnz * g.tnx;
+    for (long long q = 0; q < nplanes; ++q)
+        CK(cudaMemcpy2DAsync(out + q * cells, (size_t)g.tnx * sizeof(float),
+                             store + q * g.plane + (long long)ZO * g.pitch + XO, (size_t)g.pitch * sizeof(float),
+                             (size_t)g.tnx * sizeof(float), (size_t)g.tnz, cudaMemcpyDeviceToDevice, st));
+    return PYFWI_OK;
+}
+
 int pyfwi_frame_check(pyfwi_plan *p, void *ws, size_t bytes, int64_t *nonzero, void *stream)
 {
     if (!p || !nonzero) return fail(PYFWI_E_INVALID, "NULL argument");

@@ -139,6 +139,17 @@ class Plan:
                                            _stream(self.device)))
         return n.value
 
+    def checkpoint_states(self):
+        """pyfwi_checkpoint_states: the states a reverse-mode plan stored at
+        its checkpoint steps in the last forward call, a device tensor
+        [ns, nchp, 5, nz+2npml, nx+2npml] (fields vx, vz, taux, tauz, tauxz)."""
+        nchp = 0 if self._chp is None else int(self._chp.size)
+        tnz, tnx = self.nz + 2 * self.npml, self.nx + 2 * self.npml
+        out = torch.empty((self.ns, nchp, 5, tnz, tnx), dtype=torch.float32, device=self.device)
+        N.check(self.lib.pyfwi_checkpoint_states(self.handle, self.ws, self.ws_bytes, _ptr(out),
+                                                 _stream(self.device)))
+        return out
+
     def wait_selftest(self, limit_ns):
         """pyfwi_wait_selftest: a bounded device wait that nothing ends gives
         up after limit_ns and sets the error word (read by check_device)."""

@@ -422,7 +422,8 @@ class WavePropagator(WavePreparation):
         vp, vs, rho = (self._to_device(model0[k]) for k in ("vp", "vs", "rho"))
         self.plan.set_model(vp, vs, rho, *self._damping())
         self._traces = self.plan.forward(self._wavelet, self._traces)
-        self._model_dev = (vp, vs, rho)
+        self._model_dev = tuple(t.clone() for t in (vp, vs, rho))  # for W: the caller may edit its tensors
+        self._W, self._W_from_plan = None, self.checkpoint == "reverse"
         data = self._section(self._traces)
         self._check_device(as_numpy)
         if as_numpy:
@@ -466,6 +467,45 @@ class WavePropagator(WavePreparation):
         if self.seismo_shape == "2d":
             return data
         return {k: v.view(nt, ns, nr).permute(0, 2, 1) for k, v in data.items()}
+
+    @property
+    def W(self):
+        """The forward wavefields at the checkpoint steps ``chp``, as the
+        reference keeps them (wave_propagation.py:150-156, filled at
+        :710-727): {'vx', 'vz', 'taux', 'tauz', 'tauxz'}, each a float32
+        array (tnz, tnx, ns, nchp) whose [:, :, s, k] is the state of shot s
+        after internal step chp[k] of the last model run forward.  The
+        reference copies them to the host on every forward run; here they are
+        built on first access and kept until the next run: read from the
+        plan's checkpoint store after forward_modeling in reverse mode, else
+        from a forward run of a reverse-mode plan with the same checkpoint
+        steps.  Zeros before any forward run, as in the reference."""
+        if getattr(self, "_W", None) is not None:
+            return self._W
+        shape = (int(self.tnz), int(self.tnx), int(self.ns), int(self.nchp))
+        if getattr(self, "_model_dev", None) is None:
+            return {k: np.zeros(shape, np.float32) for k in FIELDS}
+        if self._W_from_plan:
+            states = self.plan.checkpoint_states()
+        else:
+            o = N.Options()
+            o.checkpoint = N.CKPT_REVERSE
+            o.tile, o.chunk = self.plan.opts.tile, self.plan.opts.chunk
+            try:
+                plan = Plan(self._geometry(), np.asarray(self.srcx, np.int32).reshape(-1),
+                            np.asarray(self.srcz, np.int32).reshape(-1), o, self.device,
+                            chp=np.asarray(self.chp, np.int32))
+            except torch.cuda.OutOfMemoryError as e:
+                raise MemoryError("W holds %d states of %d x %d cells per shot and field; they do not fit in "
+                                  "device memory" % (int(self.nchp), int(self.tnz), int(self.tnx))) from e
+            plan.set_model(*self._model_dev, *self._damping())
+            plan.forward(self._wavelet)
+            states = plan.checkpoint_states()
+            del plan
+        host = states.cpu().numpy()  # [ns, nchp, 5, tnz, tnx]
+        del states
+        self._W = {k: np.ascontiguousarray(host[:, :, q].transpose(2, 3, 0, 1)) for q, k in enumerate(FIELDS)}
+        return self._W
 
     @property
     def seismogram(self):
@@ -524,7 +564,8 @@ class WavePropagator(WavePreparation):
         as_numpy = not isinstance(model0["vp"], torch.Tensor)
         vp, vs, rho = (self._to_device(model0[k]) for k in ("vp", "vs", "rho"))
         self.plan.set_model(vp, vs, rho, *self._damping())
-        self._model_dev = (vp, vs, rho)
+        self._model_dev = tuple(t.clone() for t in (vp, vs, rho))  # for W: the caller may edit its tensors
+        self._W, self._W_from_plan = None, False
         nt, nrs = int(self.nt_ext), int(self.nr) * int(self.ns)
         obs = [None] * 5
         for k, v in d_obs.items():
