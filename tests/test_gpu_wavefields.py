@@ -30,7 +30,7 @@ def _check(W, g, name):
     return Wf
 
 
-@pytest.mark.parametrize("name", ["tiny_chpr", "tiny_dxr"])
+@pytest.mark.parametrize("name", ["tiny_chpr", "tiny_dxr", "tiny_dtscale", "tiny_water"])
 def test_W_matches_the_reference(name):
     g = load_golden("wavefields")
     case = cases.by_name(name)

@@ -12,7 +12,7 @@ from conftest import load_golden
 FIELDS = ("vx", "vz", "taux", "tauz", "tauxz")
 
 
-@pytest.mark.parametrize("name", ["tiny_chpr", "tiny_dxr"])
+@pytest.mark.parametrize("name", ["tiny_chpr", "tiny_dxr", "tiny_dtscale", "tiny_water"])
 def test_oracle_states_are_the_references_W(name):
     import oracle as O
     g = load_golden("wavefields")
