@@ -4,14 +4,14 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One step = one misfit-and-gradient evaluation of all shots: forward
-modelling, L2 residual against the observed data, adjoint-state gradient
-(and, for N > 1, the NCCL sum of the gradient over ranks).  Throughput is
+modelling, L2 residual against the observed data, adjoint-state gradient.  Throughput is
 grid-cell updates per second: padded cells x internal time steps x shots,
 counted once for the forward and once for the adjoint pass.
 
-With N GPUs every rank evaluates its own 64-shot survey (weak scaling) and
-the per-rank gradients are summed with one all-reduce per step.  Rank 0
-prints one JSON line.
+With N GPUs every rank evaluates its own 64-shot survey (weak scaling,
+independent replicas: the propagator runs on one GPU and nothing is
+exchanged on the data path); the step time is the maximum over ranks.
+Rank 0 prints one JSON line.
 
 --impl reference times the reference's own kernels (PyFWI's elastic.cl /
 elastic_surface.cl compiled for the host CPU; oracle/ref_driver.py) in the
@@ -130,10 +130,12 @@ def survey(ns, nt=None, config="c3"):
 # --------------------------------------------------------------------------
 # the reference arm and the CPU baseline
 # --------------------------------------------------------------------------
-def cpu_sample(case, seconds=15.0, max_steps=4000):
+def cpu_sample(case, seconds=15.0, max_steps=4000, detail=None):
     """Time the reference's kernels (or the oracle port when they are not
     built) on one shot over the first n steps, forward + backward; n is sized
-    for about `seconds` of work.  Returns (Gcell-updates/s, description)."""
+    for about `seconds` of work.  Returns (Gcell-updates/s, kind, threads,
+    description); `detail` (a dict), when given, receives the timed sample's
+    seconds, steps and cell-updates."""
     import oracle as O
     import ref_driver
     inpa = case["inpa"]
@@ -180,6 +182,8 @@ def cpu_sample(case, seconds=15.0, max_steps=4000):
         kind = "port"
         desc = ("oracle restatement (C, OpenMP, %d threads), 1 shot x first %d of %d steps, forward + backward"
                 % (threads, n, W.nt))
+    if detail is not None:
+        detail.update(seconds=t, steps=n, shots=1, cell_updates=2.0 * cells * n)
     return 2.0 * cells * n / t / 1e9, kind, threads, desc
 
 
@@ -189,16 +193,28 @@ def run_reference(args, world, rank):
         return
     for _ in range(args.warmup):
         cpu_sample(case, seconds=args.cpu_seconds / 3)
-    vals = []
+    vals, samples = [], []
     for _ in range(args.steps):
-        v, kind, cores, desc = cpu_sample(case, seconds=args.cpu_seconds)
+        detail = {}
+        v, kind, cores, desc = cpu_sample(case, seconds=args.cpu_seconds, detail=detail)
         vals.append(v)
+        samples.append(detail)
     value = statistics.median(vals)
-    cells = 2.0 * 560 * 1060 * 4000 * 64
+    # cell-updates of one step of the workload (all shots, whole record,
+    # forward + adjoint), from the survey itself
+    full = survey(64)
+    nz, nx = full["model_est"]["vp"].shape
+    npml = full["inpa"]["npml"]
+    nt = int(1 + full["inpa"]["t"] // full["inpa"]["dt"])
+    cells = 2.0 * (nz + 2 * npml) * (nx + 2 * npml) * nt * len(full["src_loc"])
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": cells / (value * 1e9) * 1e3,
+            "steps": args.steps, "warmup": args.warmup,
+            # a whole step of the workload on the host would take hours: this
+            # is the step time the measured rate implies, not a timed step
+            "ms_per_step": cells / (value * 1e9) * 1e3, "extrapolated": True,
+            "timed_samples": samples,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample": desc},
+            "config": {"workload": WORKLOAD, "sample": desc, "cell_updates_per_step": cells},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -207,6 +223,18 @@ def run_reference(args, world, rank):
 # --------------------------------------------------------------------------
 # our arm
 # --------------------------------------------------------------------------
+def max_over_ranks(ms, world, dev):
+    """The slowest rank's time: each rank's device-timed milliseconds, MAX
+    over the process group (the only collective the bench issues)."""
+    if world == 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, world, rank, local):
     import torch
     import torch.distributed as dist
@@ -231,17 +259,10 @@ def run_ours(args, world, rank, local):
     m_obs = {k: torch.from_numpy(v).to(dev) for k, v in case["model_obs"].items()}
     d_obs = {k: v.clone() for k, v in W.forward_modeling(m_obs).items()}
 
-    def allreduce(grad, rms):
-        if world > 1:
-            dist.all_reduce(grad)
-            dist.all_reduce(rms)
-
     def step(model, obs):
         # forward modelling, L2 misfit and gradient of every shot (FWI.fprime)
         rms, grad = W.misfit_gradient(model, obs, parameterization="dv")
-        g = torch.stack([grad["vp"], grad["vs"], grad["rho"]])
-        allreduce(g, rms)
-        return g, rms
+        return torch.stack([grad["vp"], grad["vs"], grad["rho"]]), rms
 
     for _ in range(args.warmup):
         step(m_est, d_obs)
@@ -269,10 +290,7 @@ def run_ours(args, world, rank, local):
     W.plan.profile(False)
     prof = {k: W.plan.profile_read(k) for k in (0, 1, 2)}
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, world, dev)
     value = world * cell_updates * args.steps / (ms_max * 1e-3) / 1e9
 
     # end to end through the public API from pinned host buffers
@@ -295,10 +313,7 @@ def run_ours(args, world, rank, local):
         rms_host.copy_(rms, non_blocking=True)
     e3.record()
     torch.cuda.synchronize()
-    t = torch.tensor([e2.elapsed_time(e3)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * cell_updates * args.steps / (float(t.item()) * 1e-3) / 1e9
+    e2e_value = world * cell_updates * args.steps / (max_over_ranks(e2.elapsed_time(e3), world, dev) * 1e-3) / 1e9
 
     if rank != 0:
         return
@@ -325,14 +340,19 @@ def run_ours(args, world, rank, local):
     else:
         alg_bytes = cells_k * bpc
     achieved = alg_bytes / (ms_k * 1e-3) / 1e9 if ms_k > 0 else None
-    traffic = None
+    traffic, traffic_src = None, None
     tp = os.path.join(ROOT, "profiles", "traffic_%s_c3.json" % name)
-    if os.path.exists(tp):
+    if os.path.exists(tp) and args.config == "c3":
         with open(tp) as f:
             tj = json.load(f)
+        # ncu DRAM bytes per cell-shot of one launch of the profile's capture,
+        # times the cell-shots of this run's average launch
         traffic = tj["dram_bytes_per_cell_shot"] * cells_k / max(n_l, 1)
+        traffic_src = {"ncu_capture": tj.get("capture"), "shots_per_launch": tj.get("shots_per_launch"),
+                       "scaled_to": "cell-shots of this run's average launch"}
     roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm if achieved else None, "traffic": traffic, "peak_source": peak_src,
+            "frac": achieved / hbm if achieved else None, "traffic": traffic, "traffic_source": traffic_src,
+            "peak_source": peak_src,
             "launches": n_l, "avg_launch_ms": ms_k / max(n_l, 1),
             "alg_bytes_per_launch": alg_bytes / max(n_l, 1),
             "kernel_share": {kinds[k][0]: prof[k][1] / max(ms, 1e-9) for k in prof}}
@@ -479,9 +499,13 @@ def configs_run(args, dev):
     """The two smaller configurations (cases.c1: 100 x 100 cells, 4 shots,
     nt 500; cases.c2: 200 x 400 cells, 10 shots, nt 2000): one misfit and
     gradient evaluation of all shots on the device (CUDA events, 3 timed
-    after 1 untimed; direct launches, and the plan replaying its captured
-    graph), and the reference's kernels on the host cores on one shot
-    (bounded sample, as cpu_baseline); Gcell-updates/s and shots/s."""
+    after 1 untimed) in four forms -- the plain form (one shot per launch
+    sequence, every step one launch issued from the host), all shots per
+    launch with launches issued from the host, the plan replaying its
+    captured graph, and the persistent time loops -- and the reference's
+    kernels on the host cores on one shot (bounded sample, as cpu_baseline);
+    Gcell-updates/s and shots/s, and the persistent form's shots/s over the
+    plain form's."""
     import cases
     import torch
     from helpers import product
@@ -489,7 +513,10 @@ def configs_run(args, dev):
     for name in ("c1", "c2"):
         case = cases.by_name(name)
         gpu = {}
-        for form, extra in (("launches", {"graph": False}), ("graph", {"graph": True})):
+        forms = (("plain", {"graph": False, "persist": False, "shot_batch": 1, "segment": 0}),
+                 ("launches", {"graph": False, "persist": False}), ("graph", {"graph": True, "persist": False}),
+                 ("persistent", {"persist": True, "shot_batch": 0, "segment": 0}))
+        for form, extra in forms:
             W = product(case, cuda_device=str(dev), **extra)
             obs = {k: v.clone() for k, v in W.forward_modeling(
                 {k: torch.from_numpy(v).to(dev) for k, v in case["model_obs"].items()}).items()}
@@ -498,6 +525,7 @@ def configs_run(args, dev):
             W.misfit_gradient(model, obs)
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            l0 = W.plan.launches()
             e0.record()
             for _ in range(3):
                 W.misfit_gradient(model, obs)
@@ -505,8 +533,12 @@ def configs_run(args, dev):
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1) / 3
             gpu[form] = {"ms_per_evaluation": ms, "value": per_shot * int(W.ns) / (ms * 1e-3) / 1e9, "unit": UNIT,
-                         "shots_per_s": int(W.ns) / (ms * 1e-3)}
+                         "shots_per_s": int(W.ns) / (ms * 1e-3),
+                         "launches_per_evaluation": (W.plan.launches() - l0) / 3,
+                         "layout": {"shot_batch": int(W.shot_batch), "segment": int(W.segment),
+                                    "persist": int(W.plan.opts.persist), "graph": int(W.plan.opts.graph)}}
             del W, obs
+        gpu["persistent_over_plain"] = gpu["persistent"]["shots_per_s"] / gpu["plain"]["shots_per_s"]
         cpu = None
         if not args.no_cpu:
             v, kind, cores, desc = cpu_sample(case, seconds=args.cpu_seconds / 3)
@@ -524,7 +556,7 @@ def plain_form(args, dev, batched_shots_s):
     import torch
     from helpers import product
     case = survey(args.plain_shots, args.nt)
-    extra = {"cuda_device": str(dev), "segment": 0, "shot_batch": 1, "graph": False}
+    extra = {"cuda_device": str(dev), "segment": 0, "shot_batch": 1, "graph": False, "persist": False}
     if args.tile is not None:
         extra["tile"] = args.tile if args.tile == "auto" else int(args.tile)
     if args.adj_tile is not None:

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PYFWI_ABI_VERSION 6
+#define PYFWI_ABI_VERSION 7
 
 enum pyfwi_status {
     PYFWI_OK = 0,
@@ -53,7 +53,11 @@ enum pyfwi_checkpoint {
     PYFWI_CKPT_REVERSE = 1
 };
 
-enum pyfwi_snapshot { PYFWI_SNAP_FP32 = 0, PYFWI_SNAP_BF16 = 1 };
+/* Format of the stored forward states the imaging reads (exact mode): FP32;
+ * BF16 (8 mantissa bits, half the store); or 24 bits (the float rounded to
+ * 15 mantissa bits, kept as a BF16 plane plus a byte plane: three quarters
+ * of the store).  The forward recurrence is FP32 in every format. */
+enum pyfwi_snapshot { PYFWI_SNAP_FP32 = 0, PYFWI_SNAP_BF16 = 1, PYFWI_SNAP_FP24 = 2 };
 
 enum pyfwi_parameterization { PYFWI_PARAM_LMD = 0, PYFWI_PARAM_DV = 1 };
 
@@ -100,25 +104,32 @@ typedef struct pyfwi_geometry {
  *   J = 1/2 sum (trace - observed)^2 of the discrete forward step of this
  *   library (transposed step, the absorbing profiles held fixed), on the whole
  *   model grid with no mask; the residual planes are dJ/dtrace per raw trace.
- *   Needs PYFWI_CKPT_EXACT and no energy terms; with PYFWI_SNAP_BF16 the
- *   transposed step reads S_{t+1} and S_t from the BF16 snapshots. */
+ *   Needs PYFWI_CKPT_EXACT and no energy terms; with PYFWI_SNAP_BF16 or
+ *   PYFWI_SNAP_FP24 the transposed step reads S_{t+1} and S_t from the
+ *   snapshots. */
 enum pyfwi_adjoint { PYFWI_ADJOINT_REFERENCE = 0, PYFWI_ADJOINT_EXACT = 1 };
 
 typedef struct pyfwi_options {
     int32_t checkpoint;     /* enum pyfwi_checkpoint */
     int32_t segment;        /* exact mode: steps per recompute segment; 0 = all steps */
-    int32_t snapshot;       /* exact mode: enum pyfwi_snapshot for stored states */
+    int32_t snapshot;       /* exact mode: enum pyfwi_snapshot for the imaged states */
     int32_t shot_batch;     /* shots propagated together; 0 = all */
     int32_t energy;         /* 1: also accumulate the energy terms (energy_balancing) */
     int32_t nchp;           /* reverse mode: number of checkpoint steps */
     const int32_t *chp;     /* host; reverse mode: the checkpoint steps (copied) */
     int32_t tile;           /* kernel variant (see pyfwi_tile_count): 0..2 tile kernels with
                                16 / 8 / 32 rows per tile, 3..5 streaming kernels with
-                               128 / 64 / 256 columns per CTA */
+                               128 / 64 / 256 columns per CTA, 6..7 16-row tile kernels
+                               whose adjoint CTAs carry 2 / 4 shots (forward as 0) */
     int32_t graph;          /* 1: replay time loops as CUDA graphs */
     int32_t chunk;          /* streaming kernels: grid rows per CTA, 0 = from the grid size */
     int32_t adj_tile;       /* adjoint+imaging step variant + 1 (same numbering as tile); 0 = tile */
     int32_t adjoint;        /* enum pyfwi_adjoint */
+    int32_t persist;        /* 1: run the time loops of small surveys as persistent cooperative
+                               kernels (many steps per launch, a grid barrier between steps)
+                               where the layout allows: exact checkpoints holding every step in
+                               FP32, the tile kernels (variants 0..2), the reference adjoint;
+                               otherwise (and inside a caller's stream capture) one launch per step */
 } pyfwi_options;
 
 typedef struct pyfwi_plan pyfwi_plan;
@@ -199,14 +210,19 @@ int pyfwi_misfit_gradient(pyfwi_plan *plan, void *workspace, size_t bytes, const
                           int32_t parameterization, float *traces, float *grad, double *misfit, void *stream);
 
 /* Low-pass filter of the multiscale misfit (lowpass / adj_lowpass,
- * fwi_tools.py:1188-1258): each of n_planes device planes [nt][ncols] of
- * traces (time along rows) is multiplied along time by `response`, the
- * device nt x nt matrix of the filter (symmetric; built on the host from the
- * Butterworth design, pyfwi_b200.fwi_tools.lowpass_response), as an FP32
- * GEMM.  in and out must not overlap.  Uses one cuBLAS handle per calling
- * thread and device, created on first use. */
-int pyfwi_lowpass(const float *response, const float *in, float *out, int32_t nt, int64_t ncols, int32_t n_planes,
-                  void *stream);
+ * fwi_tools.py:1188-1258): every trace (column) of n_planes device planes
+ * [nt][ncols] (time along rows) is convolved along time with the filter's
+ * symmetric impulse response g, y[t] = sum_s g[|t - s|] x[s], by FFTs of
+ * nfft points on the device.
+ *   filter  device float[2 * nfft]: the real spectrum of the response
+ *           embedded in a circulant of nfft points, 1/nfft included
+ *           (filter[0..nfft)), then the twiddles exp(-2 pi i j / nfft),
+ *           j < nfft / 2, as (cos, sin) pairs; built on the host from the
+ *           Butterworth design (pyfwi_b200.fwi_tools.lowpass_spectrum)
+ *   nfft    a power of two with 2 nt - 1 <= nfft <= 16384 (nt <= 8192)
+ * in and out must not overlap.  Allocates nothing; one kernel launch. */
+int pyfwi_lowpass(const float *filter, int32_t nfft, const float *in, float *out, int32_t nt, int64_t ncols,
+                  int32_t n_planes, void *stream);
 
 /* Trace section (acquisition.py:313-333): out = (a + b) / 2 elementwise. */
 int pyfwi_mean2(const float *a, const float *b, float *out, int64_t n, void *stream);
@@ -238,7 +254,9 @@ int pyfwi_launch_count(const pyfwi_plan *plan, int64_t *count);
 /* Read and clear the workspace's device error word after the work queued on
  * `stream` (synchronises that stream).  *code: 0 none, 1 a streaming kernel
  * gave up waiting (one second) for a row copy and left its rows unwritten,
- * 2 a streaming kernel found its shared memory misaligned for copies.
+ * 2 a streaming kernel found its shared memory misaligned for copies, 3 a
+ * persistent kernel gave up waiting (one second) at a grid barrier and left
+ * its remaining steps undone.
  * Returns PYFWI_E_TIMEOUT when *code != 0.  The reference has no device-side
  * waits and no counterpart. */
 int pyfwi_device_error(pyfwi_plan *plan, void *workspace, size_t bytes, int32_t *code, void *stream);
@@ -269,6 +287,14 @@ int pyfwi_frame_check(pyfwi_plan *plan, void *workspace, size_t bytes, int64_t *
  * reference counterpart. */
 int pyfwi_wait_selftest(pyfwi_plan *plan, void *workspace, size_t bytes, int64_t limit_ns, void *stream);
 
+/* Failure-path self test of the persistent kernels' grid barrier: two CTAs
+ * wait at the barrier for a third that does not exist, with the wait cut to
+ * `limit_ns` (1e3 .. 1e10) of the GPU's global timer, then give up as a
+ * persistent kernel does and set the workspace's error word to 3.  Until
+ * pyfwi_device_error reads and clears the word, the persistent kernels of
+ * later calls stop at their first barrier.  No reference counterpart. */
+int pyfwi_barrier_selftest(pyfwi_plan *plan, void *workspace, size_t bytes, int64_t limit_ns, void *stream);
+
 /* Gradient evaluation that allocates no device memory.  No counterpart in
  * the reference (PyFWI allocates its buffers through pyopencl per
  * WavePropagator).  For callers that cannot call cudaMalloc -- e.g. a host
@@ -285,8 +311,10 @@ int pyfwi_wait_selftest(pyfwi_plan *plan, void *workspace, size_t bytes, int64_t
  * Plans whose workspace + traces + residuals exceed the array are rejected
  * (PYFWI_E_WORKSPACE, message gives the bytes needed).  The first call on a
  * device looks up the array's device address; make it before any stream
- * capture.  All calls on a device share the array (each call clears what it
- * needs); calls that overlap on the GPU race. */
+ * capture.  That address is kept until the process exits: after a
+ * cudaDeviceReset of the device, do not call this entry point again in the
+ * same process.  All calls on a device share the array (each call clears
+ * what it needs); calls that overlap on the GPU race. */
 #define PYFWI_STATIC_SCRATCH_BYTES (64u << 20)
 int pyfwi_gradient_static(pyfwi_plan *plan, const float *vp, const float *vs, const float *rho,
                           const float *damp_x, const float *damp_z, const float *src_vals, int32_t n_src,

@@ -13,7 +13,7 @@ _P = ctypes.c_void_p
 
 PYFWI_OK = 0
 CKPT_EXACT, CKPT_REVERSE = 0, 1
-SNAP_FP32, SNAP_BF16 = 0, 1
+SNAP_FP32, SNAP_BF16, SNAP_FP24 = 0, 1, 2
 ADJOINT_REFERENCE, ADJOINT_EXACT = 0, 1
 PARAM_LMD, PARAM_DV = 0, 1
 
@@ -30,14 +30,14 @@ class Geometry(ctypes.Structure):
                 ("mask_row0", _i32), ("mask_row1", _i32), ("mask_col0", _i32), ("mask_col1", _i32)]
 
 
-ABI_VERSION = 6  # PYFWI_ABI_VERSION of include/pyfwi_b200.h
+ABI_VERSION = 7  # PYFWI_ABI_VERSION of include/pyfwi_b200.h
 REDUCE_SLOTS = 2368  # PYFWI_REDUCE_SLOTS
 
 
 class Options(ctypes.Structure):
     _fields_ = [("checkpoint", _i32), ("segment", _i32), ("snapshot", _i32), ("shot_batch", _i32), ("energy", _i32),
                 ("nchp", _i32), ("chp", ctypes.POINTER(_i32)), ("tile", _i32), ("graph", _i32), ("chunk", _i32),
-                ("adj_tile", _i32), ("adjoint", _i32)]
+                ("adj_tile", _i32), ("adjoint", _i32), ("persist", _i32)]
 
 
 class NativeError(RuntimeError):
@@ -67,12 +67,13 @@ def lib():
     L.pyfwi_mean2.argtypes = [_P, _P, _P, ctypes.c_int64, _P]
     L.pyfwi_misfit_gradient.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_float), _i32,
                                         ctypes.POINTER(_P), _i32, ctypes.POINTER(_P), _i32, _P, _P, _P, _P]
-    L.pyfwi_lowpass.argtypes = [_P, _P, _P, _i32, ctypes.c_int64, _i32, _P]
+    L.pyfwi_lowpass.argtypes = [_P, _i32, _P, _P, _i32, ctypes.c_int64, _i32, _P]
     L.pyfwi_smooth.argtypes = [_P, _P, _P, _i32, _i32, _i32, ctypes.POINTER(ctypes.c_double), _i32, _P]
     L.pyfwi_tile_count.argtypes = [_i32]
     L.pyfwi_launch_count.argtypes = [_P, ctypes.POINTER(ctypes.c_int64)]
     L.pyfwi_device_error.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(_i32), _P]
     L.pyfwi_wait_selftest.argtypes = [_P, _P, ctypes.c_size_t, ctypes.c_int64, _P]
+    L.pyfwi_barrier_selftest.argtypes = [_P, _P, ctypes.c_size_t, ctypes.c_int64, _P]
     L.pyfwi_frame_check.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int64), _P]
     L.pyfwi_checkpoint_states.argtypes = [_P, _P, ctypes.c_size_t, _P, _P]
     L.pyfwi_profile_enable.argtypes = [_P, _i32]
@@ -86,7 +87,7 @@ def lib():
     for name in ("pyfwi_plan_create", "pyfwi_plan_destroy", "pyfwi_workspace_size", "pyfwi_set_model",
                  "pyfwi_forward", "pyfwi_gradient", "pyfwi_l2_residual", "pyfwi_mean2", "pyfwi_tile_count",
                  "pyfwi_launch_count", "pyfwi_profile_enable", "pyfwi_profile_read", "pyfwi_device_error",
-                 "pyfwi_smooth", "pyfwi_misfit_gradient", "pyfwi_lowpass", "pyfwi_wait_selftest",
+                 "pyfwi_smooth", "pyfwi_misfit_gradient", "pyfwi_lowpass", "pyfwi_wait_selftest", "pyfwi_barrier_selftest",
                  "pyfwi_frame_check", "pyfwi_checkpoint_states"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L

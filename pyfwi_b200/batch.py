@@ -33,6 +33,12 @@ class SurveyBatch:
         if any(torch.device(W.device) != self.device for W in self.props):
             raise ValueError("every survey of a batch must be on one device")
         self.streams = [torch.cuda.Stream(self.device) for _ in self.props]
+        # the surveys run side by side: each keeps one launch per step (a
+        # persistent cooperative grid per survey would compete for the SMs)
+        for W in self.props:
+            W.persist_allowed = False
+            if W._plan is not None and W._plan.opts.persist:
+                W._plan = None  # rebuilt on first use, without persistent loops
         self._share_memory()
         self.graph = graph
         self._graph = None

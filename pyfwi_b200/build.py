@@ -37,7 +37,7 @@ def build(force=False, verbose=False):
     if not force and up_to_date():
         return LIB
     tmp = LIB + ".tmp%d" % os.getpid()
-    cmd = [nvcc()] + NVCC_FLAGS + SOURCES + ["-lcublas", "-o", tmp]
+    cmd = [nvcc()] + NVCC_FLAGS + SOURCES + ["-o", tmp]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)

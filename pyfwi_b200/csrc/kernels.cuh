@@ -63,6 +63,16 @@ __device__ __forceinline__ float4 ld4(const float *plane, const Grid &g, int gi,
     return __ldg(reinterpret_cast<const float4 *>(plane + (long long)ar * g.pitch + ac));
 }
 
+// ld4 through L2 only (ld.global.cg): for data other CTAs of the same
+// launch wrote (the persistent kernels), which the read-only path may hold
+// stale.
+__device__ __forceinline__ float4 ld4c(const float *plane, const Grid &g, int gi, int gj)
+{
+    int ar = gi + ZO, ac = gj + XO;
+    if (ar < 0 || ar >= g.rows || ac < 0 || ac + 3 >= g.pitch) return make_float4(0.f, 0.f, 0.f, 0.f);
+    return __ldcg(reinterpret_cast<const float4 *>(plane + (long long)ar * g.pitch + ac));
+}
+
 __device__ __forceinline__ void st4s(float *s, float4 v) { *reinterpret_cast<float4 *>(s) = v; }
 
 // Asynchronous 16-byte copy of the 4 cells (gi, gj .. gj+3) of `plane` into
@@ -217,12 +227,27 @@ __device__ __forceinline__ float gbwd(const float *f, long long i, long long s, 
 }
 
 // The same differences with the values taken through a loader ld(index):
-// a BF16 snapshot plane widened to float, or an FP32 plane rounded to BF16
-// first (so that every forward state the BF16 exact adjoint reads carries
-// the same rounding, whichever slot holds it).
-__device__ __forceinline__ float ldh(const __nv_bfloat16 *f, long long i)
+// a snapshot plane widened to float, or an FP32 plane rounded to the
+// snapshot format first (so that every forward state the exact adjoint
+// reads from snapshots carries the same rounding, whichever slot holds it).
+
+// 24-bit snapshots: the 24 leading bits of a float (sign, exponent, 15
+// mantissa bits) rounded to nearest even, kept as a BF16 plane (the upper 16
+// bits) and a byte plane (the next 8).  A BF16 snapshot is the same with no
+// byte plane (rounded to its 16 bits instead).
+__device__ __forceinline__ unsigned fp24_bits(float v)
 {
-    return __bfloat162float(__ushort_as_bfloat16(__ldg(reinterpret_cast<const unsigned short *>(f) + i)));
+    const unsigned u = __float_as_uint(v);
+    return (u + 0x7Fu + ((u >> 8) & 1u)) >> 8;
+}
+
+__device__ __forceinline__ float fp24_round(float v) { return __uint_as_float(fp24_bits(v) << 8); }
+
+// Snapshot value i: BF16 plane h, widened with byte plane l when l is set.
+__device__ __forceinline__ float snapv(const __nv_bfloat16 *h, const unsigned char *l, long long i)
+{
+    const unsigned hi = reinterpret_cast<const unsigned short *>(h)[i];
+    return __uint_as_float((hi << 16) | (l ? (unsigned)l[i] << 8 : 0u));
 }
 
 template <int R, typename L>
@@ -292,21 +317,34 @@ struct StepArgs {
     Lines lines;
     int chunk;             // streaming kernels: grid rows per CTA
     __nv_bfloat16 *snap;   // nullable: BF16 copy of the output state, slot 0
+    unsigned char *snap8;  // nullable: the byte planes of a 24-bit snapshot (snap holds the upper 16 bits)
     long long snap_stride; // elements between the snapshots of consecutive slots
     const float *tbase;    // streaming kernels: workspace base = row 0 of `tmap`
     int *err;              // streaming kernels: workspace error word
     alignas(64) CUtensorMap tmap;  // streaming kernels: the workspace as rows of `pitch` floats
 };
 
-// BF16 copy of the five fields written at cell `co` (round to nearest even).
-__device__ __forceinline__ void write_snap(__nv_bfloat16 *sn, long long P, long long co, float vx, float vz, float txx,
-                                           float tzz, float txz)
+// Snapshot of the five fields written at cell `co` (round to nearest even):
+// BF16, or 24 bits when the byte planes sn8 are given.
+__device__ __forceinline__ void write_snap1(__nv_bfloat16 *sn, unsigned char *sn8, long long o, float v)
 {
-    sn[VX * P + co] = __float2bfloat16_rn(vx);
-    sn[VZ * P + co] = __float2bfloat16_rn(vz);
-    sn[TXX * P + co] = __float2bfloat16_rn(txx);
-    sn[TZZ * P + co] = __float2bfloat16_rn(tzz);
-    sn[TXZ * P + co] = __float2bfloat16_rn(txz);
+    if (sn8) {
+        const unsigned b = fp24_bits(v);
+        sn[o] = __ushort_as_bfloat16((unsigned short)(b >> 8));
+        sn8[o] = (unsigned char)(b & 0xFFu);
+    } else {
+        sn[o] = __float2bfloat16_rn(v);
+    }
+}
+
+__device__ __forceinline__ void write_snap(__nv_bfloat16 *sn, unsigned char *sn8, long long P, long long co, float vx,
+                                           float vz, float txx, float tzz, float txz)
+{
+    write_snap1(sn, sn8, VX * P + co, vx);
+    write_snap1(sn, sn8, VZ * P + co, vz);
+    write_snap1(sn, sn8, TXX * P + co, txx);
+    write_snap1(sn, sn8, TZZ * P + co, tzz);
+    write_snap1(sn, sn8, TXZ * P + co, txz);
 }
 
 struct AdjArgs {
@@ -317,6 +355,7 @@ struct AdjArgs {
     long long in_stride, out_stride;
     const float *fwd;      // forward state S_{t+1}, slot 0 (FP32)
     const __nv_bfloat16 *fwd16;  // same, BF16 snapshot (used when fwd == nullptr)
+    const unsigned char *fwd8;   // nullable: byte planes of a 24-bit snapshot (with fwd16)
     long long fwd_stride;
     float *gacc;           // [slot][3 or 6][plane] accumulators
     long long gacc_stride;
@@ -330,6 +369,7 @@ struct AdjArgs {
     int nr, ns;
     Lines lines;
     int chunk;             // streaming kernels: grid rows per CTA
+    int nslots;            // tile kernel: shots in this launch (CTAs of blockIdx.z carry NS of them)
     const float *tbase;    // streaming kernels: workspace base = row 0 of `tmap`
     int *err;              // streaming kernels: workspace error word
     alignas(64) CUtensorMap tmap;  // streaming kernels: the workspace as rows of `pitch` floats
@@ -356,9 +396,9 @@ __device__ __forceinline__ int line_slot(const Lines &L, int l, int i, int j)
     return d < L.count[l] ? d : -1;
 }
 
-// Record the five fields of `st` at cell (i, j) into every trace slot whose
-// receiver sits there.
-__device__ __forceinline__ void record_cell(const StepArgs &a, const float *st, int shot, int i, int j)
+// Record the five fields of `st` at cell (i, j) into trace row `rec_row` of
+// every trace slot whose receiver sits there.
+__device__ __forceinline__ void record_cell(const StepArgs &a, int rec_row, const float *st, int shot, int i, int j)
 {
     const Lines &L = a.lines;
     for (int l = 0; l < L.n; ++l) {
@@ -373,7 +413,7 @@ __device__ __forceinline__ void record_cell(const StepArgs &a, const float *st, 
             k = d / L.drow[l];
         }
         if (k >= L.count[l]) continue;
-        long long o = (long long)a.rec_row * a.ns * a.nr + (long long)shot * a.nr + L.slot0[l] + k;
+        long long o = (long long)rec_row * a.ns * a.nr + (long long)shot * a.nr + L.slot0[l] + k;
         long long c = cell_off(a.g, i, j);
         float vx = st[VX * a.g.plane + c];
         a.traces[0 * a.trace_plane + o] = vx;
@@ -485,23 +525,41 @@ __device__ __forceinline__ float4 damp4(const float *dampx, const Grid &g, int j
     return v;
 }
 
-template <int R, int TZ>
-__global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ StepArgs a)
+// What changes from one forward step to the next: the input and output
+// states (slot 0 and the element stride between slots), the source sample
+// and the trace row recorded (-1: none), the snapshot planes written.
+// StepArgs has the same fields: the step kernel passes its arguments
+// themselves (read from parameter space where they are used).
+struct StepVar {
+    const float *in;
+    float *out;
+    long long in_stride, out_stride;
+    float4 src;
+    int add_src;
+    int rec_row;
+    __nv_bfloat16 *snap;
+    unsigned char *snap8;
+};
+
+// One forward step of tile (bx, by) of slot `slot`; sm: FwdShape::FLOATS
+// floats of shared memory.  Ends with shared memory still in use: a caller
+// that reuses it for another tile synchronises first.
+// W24: snapshots are written as 24 bits (sv.snap8 set), else as BF16.
+template <int R, int TZ, bool W24, class V>
+__device__ __forceinline__ void fwd_tile(const StepArgs &a, const V &sv, int bx, int by, int slot, float *sm)
 {
     using S = FwdShape<R, TZ>;
     constexpr int SW = S::SW, VW = S::VW, HT = S::HT, HV = S::HV;
-    extern __shared__ float4 smem4[];
-    float *sm = reinterpret_cast<float *>(smem4);
     float *s_txx = sm, *s_tzz = s_txx + HT * SW, *s_txz = s_tzz + HT * SW;
     float *s_vx = s_txz + HT * SW, *s_vz = s_vx + HV * VW, *s_b = s_vz + HV * VW;
     float *s_lam = s_b + HV * VW, *s_mu = s_lam + TZ * TX;  // the tile's cells
 
     const Grid &g = a.g;
     const long long P = g.plane;
-    const int slot = blockIdx.z, shot = a.shot0 + slot;
-    const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TZ;
-    const float *in = a.in + slot * a.in_stride;
-    float *out = a.out + slot * a.out_stride;
+    const int shot = a.shot0 + slot;
+    const int j0 = bx * TX, i0 = by * TZ;
+    const float *in = sv.in + slot * sv.in_stride;
+    float *out = sv.out + slot * sv.out_stride;
     const int tid = threadIdx.x;
     const float dt = a.k.dt;
 
@@ -527,16 +585,16 @@ __global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ Ste
     }
     cp_wait_all();
     __syncthreads();
-    if (a.add_src && tid == 0) {  // wave_propagation.py:652-664, elastic_surface.cl:23-28
+    if (sv.add_src && tid == 0) {  // wave_propagation.py:652-664, elastic_surface.cl:23-28
         const int si = a.srcz[shot], sj = a.srcx[shot];
         const int ct = sj - (j0 - 8), cv = sj - (j0 - 4), rt = si - (i0 - 2 * R), rv = si - (i0 - R);
         if (ct >= 0 && ct < SW && rt >= 0 && rt < HT) {
-            s_txx[rt * SW + ct] += a.src.z;
-            s_tzz[rt * SW + ct] += a.src.w;
+            s_txx[rt * SW + ct] += sv.src.z;
+            s_tzz[rt * SW + ct] += sv.src.w;
         }
         if (cv >= 0 && cv < VW && rv >= 0 && rv < HV) {
-            s_vx[rv * VW + cv] += a.src.x;
-            s_vz[rv * VW + cv] += a.src.y;
+            s_vx[rv * VW + cv] += sv.src.x;
+            s_vz[rv * VW + cv] += sv.src.y;
         }
     }
     __syncthreads();
@@ -649,11 +707,19 @@ __global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ Ste
             }
         }
         for (int k = 0; k < 4 && gj + k < g.tnx; ++k) {
-            if (a.snap)
-                write_snap(a.snap + slot * a.snap_stride, P, co + k, f4(vxc, k), f4(vzc, k), oxx[k], ozz[k], oxz[k]);
-            if (a.rec_row >= 0) record_cell(a, in, shot, gi, gj + k);
+            if (sv.snap)
+                write_snap(sv.snap + slot * a.snap_stride, W24 ? sv.snap8 + slot * a.snap_stride : nullptr, P,
+                           co + k, f4(vxc, k), f4(vzc, k), oxx[k], ozz[k], oxz[k]);
+            if (sv.rec_row >= 0) record_cell(a, sv.rec_row, in, shot, gi, gj + k);
         }
     }
+}
+
+template <int R, int TZ, bool W24>
+__global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ StepArgs a)
+{
+    extern __shared__ float4 smem4[];
+    fwd_tile<R, TZ, W24>(a, a, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<float *>(smem4));
 }
 
 // ---------------------------------------------------------------------------
@@ -795,19 +861,18 @@ struct AdjShape {
     static constexpr int FLOATS = 2 * HT * W + 3 * HV * W;
 };
 
-__device__ __forceinline__ float bf(const __nv_bfloat16 *p, long long i) { return __bfloat162float(p[i]); }
 
-// The next step's residual row (AdjArgs.epi_row) added at cell (i, j) of
+// The next step's residual row epi_row added at cell (i, j) of
 // the output: to the adjoint velocities in registers and the stresses in
 // memory, one receiver line after another.
-__device__ __forceinline__ void inject_epilogue(const AdjArgs &a, int slot, int i, int j, long long co, float &avx,
+__device__ __forceinline__ void inject_epilogue(const AdjArgs &a, int epi_row, int slot, int i, int j, long long co, float &avx,
                                                 float &avz, float *out)
 {
     const long long P = a.g.plane;
     for (int l = 0; l < a.lines.n; ++l) {
         const int ks = line_slot(a.lines, l, i, j);
         if (ks < 0) continue;
-        const long long o = (long long)a.epi_row * a.ns * a.nr + (long long)(a.shot0 + slot) * a.nr + a.lines.slot0[l] + ks;
+        const long long o = (long long)epi_row * a.ns * a.nr + (long long)(a.shot0 + slot) * a.nr + a.lines.slot0[l] + ks;
         if (a.res[0]) avx += __ldg(a.res[0] + o);
         if (a.res[1]) avz += __ldg(a.res[1] + o);
         for (int f = TXX; f <= TXZ; ++f)
@@ -815,13 +880,55 @@ __device__ __forceinline__ void inject_epilogue(const AdjArgs &a, int slot, int 
     }
 }
 
-template <int R, int TZ, bool ENERGY>
-__global__ void __launch_bounds__(NTHREADS, (R == 2 && !ENERGY) ? 6 : 1) adj_step(const __grid_constant__ AdjArgs a)
+// CTAs per SM the adjoint step is built for (the register bound of its
+// launch): 6 with one shot per CTA (40 registers, 31 KB of shared memory),
+// 5 when each CTA carries NS > 1 shots (their summed accumulators take
+// another 12 KB of shared memory).
+template <int R, bool ENERGY, int NS>
+struct AdjOccupancy {
+    static constexpr int value = (R == 2 && !ENERGY) ? (NS == 1 ? 6 : NS == 2 ? 5 : 4) : 1;
+};
+
+// Shared-memory floats of the adjoint step: the staged fields, plus the
+// CTA's accumulators when it carries several shots.
+template <int R, int TZ, bool ENERGY, int NS>
+constexpr int adj_smem_floats()
+{
+    return AdjShape<R, TZ>::FLOATS + (NS > 1 ? (ENERGY ? 6 : 3) * TZ * TX : 0);
+}
+
+// One adjoint step of NS shots per CTA (blockIdx.z covers slots
+// blockIdx.z * NS ..): the shots of a CTA run one after another over the
+// same tile and add their imaging into accumulator slot blockIdx.z.  With
+// NS > 1 the accumulators of the tile's cells stay in shared memory across
+// the shots (each thread owns its cells' entries) and are read and written
+// in global memory once, instead of once per shot; the sums run in shot
+// order, then over slots in the final reduction.
+// What changes from one adjoint step to the next: the input and output
+// adjoint states, the forward state S(t+1) the imaging reads (FP32, or a
+// BF16 / 24-bit snapshot), and the residual row the next step injects.
+// AdjArgs has the same fields: the step kernel passes its arguments
+// themselves.
+struct AdjVar {
+    const float *in;
+    float *out;
+    const float *fwd;
+    const __nv_bfloat16 *fwd16;
+    const unsigned char *fwd8;
+    int epi_row;
+};
+
+// One adjoint step of tile (bx, by) for the slots bz * NS ..; sm:
+// adj_smem_floats floats of shared memory.  Ends with shared memory still in
+// use: a caller that reuses it for another tile synchronises first.
+// COH: the input adjoint state and the accumulators are read through L2
+// (written by other CTAs of the same launch: the persistent kernel).
+template <int R, int TZ, bool ENERGY, int NS, bool NARROW, bool COH, class V>
+__device__ __forceinline__ void adj_tile(const AdjArgs &a, const V &av, int bx, int by, int bz, float *sm)
 {
     using S = AdjShape<R, TZ>;
     constexpr int W = S::W, HT = S::HT, HV = S::HV, VW = TX + 2 * R;
-    extern __shared__ float4 smem4[];
-    float *sm = reinterpret_cast<float *>(smem4);
+    constexpr int NACC = ENERGY ? 6 : 3;
     // rows i0-2R ..: b*Avx and b*Avz (the operands of the adjoint stress
     // differences); after the stress update they hold lam*Atx and
     // (lam+2mu)*Atz on rows i0-R ..
@@ -832,149 +939,170 @@ __global__ void __launch_bounds__(NTHREADS, (R == 2 && !ENERGY) ? 6 : 1) adj_ste
 
     const Grid &g = a.g;
     const long long P = g.plane;
-    const int slot = blockIdx.z;
-    const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TZ, sx0 = j0 - 2 * R;
-    const float *in = a.in + slot * a.in_stride;
-    float *out = a.out + slot * a.out_stride;
+    const int j0 = bx * TX, i0 = by * TZ, sx0 = j0 - 2 * R;
     const int tid = threadIdx.x;
     const float dt = a.k.dt;
 
-    // the stresses as asynchronous copies, in flight while the velocity
-    // products are loaded and stored
-    for (int e = tid; e < HV * (W / 4); e += NTHREADS) {
-        int r = e / (W / 4), q = e - r * (W / 4);
-        int gi = i0 - R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
-        cp4(s_atx + o, in + TXX * P, g, gi, gj);
-        cp4(s_atz + o, in + TZZ * P, g, gi, gj);
-        cp4(s_atxz + o, in + TXZ * P, g, gi, gj);
-    }
-    for (int e = tid; e < HT * (W / 4); e += NTHREADS) {
-        int r = e / (W / 4), q = e - r * (W / 4);
-        int gi = i0 - 2 * R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
-        const float4 b = ld4(a.mat + 2 * P, g, gi, gj), vx = ld4(in + VX * P, g, gi, gj),
-                     vz = ld4(in + VZ * P, g, gi, gj);
-        st4s(s_pvx + o, make_float4(vx.x * b.x, vx.y * b.y, vx.z * b.z, vx.w * b.w));
-        st4s(s_pvz + o, make_float4(vz.x * b.x, vz.y * b.y, vz.z * b.z, vz.w * b.w));
-    }
-    cp_wait_all();
-    __syncthreads();
-
-    // adjoint stresses on the tile plus an R-cell ring (Adj_update_tau); the
-    // tile's own cells go straight to the output
-    for (int e = tid; e < HV * VW; e += NTHREADS) {
-        int r = e / VW, cc = e - r * VW;
-        int gi = i0 - R + r, gj = j0 - R + cc;
-        int is = r * W + cc + R, iv = is + R * W;
-        const bool tile = r >= R && r < R + TZ && cc >= R && cc < R + TX && gi < g.tnz && gj < g.tnx;
-        float atx = s_atx[is], atz = s_atz[is], atxz = s_atxz[is];
-        if (in_domain(g, R, gi, gj)) {
-            float dx = __ldg(a.dampx + gj + XO), dz = __ldg(a.dampz + gi + ZO);
-            atx = atx + (-dt) * (dx * atx + dfwd<R>(s_pvx, iv, 1, a.k.cx));
-            atz = atz + (-dt) * (dz * atz + dbwd<R>(s_pvz, iv, W, a.k.cz));
-            atxz = atxz + (-dt) * ((dx + dz) * atxz + (dfwd<R>(s_pvx, iv, W, a.k.cz) + dbwd<R>(s_pvz, iv, 1, a.k.cx)));
-            s_atx[is] = atx;
-            s_atz[is] = atz;
-            s_atxz[is] = atxz;
-        }
-        if (tile) {
-            const long long co = cell_off(g, gi, gj);
-            out[TXX * P + co] = atx;
-            out[TZZ * P + co] = atz;
-            out[TXZ * P + co] = atxz;
-        }
-    }
-    __syncthreads();
-
-    // material products of the new adjoint stresses
-    for (int e = tid; e < HV * VW; e += NTHREADS) {
-        int r = e / VW, cc = e - r * VW;
-        int gi = i0 - R + r, gj = j0 - R + cc;
-        int is = r * W + cc + R;
-        // lam = mu = 0 in the zero frame and beyond the allocated rows / columns
-        const bool alloc = gi + ZO >= 0 && gi + ZO < g.rows && gj + XO >= 0 && gj + XO < g.pitch;
-        const long long co = alloc ? cell_off(g, gi, gj) : 0;
-        const float lam = alloc ? __ldg(a.mat + co) : 0.f, mu = alloc ? __ldg(a.mat + P + co) : 0.f;
-        const float l2m = lam + 2.f * mu;
-        const float atx = s_atx[is], atz = s_atz[is], atxz = s_atxz[is];
-        s_atx[is] = l2m * atx;
-        s_atz[is] = lam * atz;
-        s_atxz[is] = mu * atxz;
-        s_pvx[is] = lam * atx;
-        s_pvz[is] = l2m * atz;
-    }
-    __syncthreads();
-
-    // adjoint velocities on the tile (Adj_update_v) and imaging (Grad)
+    // adjoint velocities and imaging: each thread takes NK consecutive rows
+    // of one column, so the z differences of the imaging slide down register
+    // windows (rows gi-R .. gi+R of the forward vz, tzz and txz): one new
+    // row per field and cell
+    constexpr int NK = TZ / (NTHREADS / TX);
     const int c = tid % TX;
     const int gj = j0 + c;
-    if (gj >= g.tnx) return;
-    const int glo = a.npml + R;
-    const float *F = a.fwd ? a.fwd + slot * a.fwd_stride : nullptr;
-    const __nv_bfloat16 *F16 = a.fwd16 ? a.fwd16 + slot * a.fwd_stride : nullptr;
-    float *G = a.gacc + slot * a.gacc_stride;
-    // each thread takes NK consecutive rows of its column, so the z
-    // differences of the imaging slide down register windows (rows gi-R ..
-    // gi+R of the forward vz, tzz and txz): one new row per field and cell
-    constexpr int NK = TZ / (NTHREADS / TX);
     const int r0 = (tid / TX) * NK;
-    const long long pz = g.pitch;
-    float wvz[2 * R + 1], wtz[2 * R + 1], wtxz[2 * R + 1];
-    const bool win = F && gj >= glo && gj <= g.tnx - R - a.npml && i0 + r0 + NK - 1 >= glo &&
-                     i0 + r0 <= g.tnz - R - a.npml;
-    if (win) {
-        const long long c0 = cell_off(g, i0 + r0, gj);
+    const int glo = a.npml + R;
+    const bool col_img = gj >= glo && gj <= g.tnx - R - a.npml;  // this column is imaged (Grad's domain)
+    float *G = a.gacc + bz * a.gacc_stride;
+    // NS > 1: the CTA's shots summed in shared memory, [NACC][TZ][TX]
+    float *s_acc = s_atxz + HV * W;
+    if (NS > 1) {
+        for (int k = 0; k < NK; ++k) {
+            const int gi = i0 + r0 + k;
+            const bool im = col_img && gi >= glo && gi <= g.tnz - R - a.npml;
+            const long long co = im ? cell_off(g, gi, gj) : 0;
 #pragma unroll
-        for (int m = 0; m < 2 * R; ++m) {
-            const long long o = c0 + (m - R) * pz;
-            wvz[m + 1] = __ldg(F + VZ * P + o);
-            wtz[m + 1] = __ldg(F + TZZ * P + o);
-            wtxz[m + 1] = __ldg(F + TXZ * P + o);
+            for (int f = 0; f < NACC; ++f) s_acc[(f * TZ + r0 + k) * TX + c] = im ? G[f * P + co] : 0.f;
         }
     }
-    for (int k = 0; k < NK; ++k) {
-        const int r = r0 + k, gi = i0 + r;
-        if (gi >= g.tnz) break;
-        int is = (r + R) * W + c + 2 * R;
-        long long co = cell_off(g, gi, gj);
-        if (win) {  // the window moves to rows gi-R .. gi+R
-            const long long o = co + R * pz;
-            shift(wvz, __ldg(F + VZ * P + o));
-            shift(wtz, __ldg(F + TZZ * P + o));
-            shift(wtxz, __ldg(F + TXZ * P + o));
+
+    for (int q = 0; q < NS; ++q) {
+        const int slot = bz * NS + q;
+        if (slot >= a.nslots) break;  // the same for every thread of the CTA
+        if (q) __syncthreads();       // the previous shot is done with shared memory
+        const float *in = av.in + slot * a.in_stride;
+        float *out = av.out + slot * a.out_stride;
+
+        // the stresses as asynchronous copies, in flight while the velocity
+        // products are loaded and stored
+        for (int e = tid; e < HV * (W / 4); e += NTHREADS) {
+            int r = e / (W / 4), q = e - r * (W / 4);
+            int gi = i0 - R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
+            cp4(s_atx + o, in + TXX * P, g, gi, gj);
+            cp4(s_atz + o, in + TZZ * P, g, gi, gj);
+            cp4(s_atxz + o, in + TXZ * P, g, gi, gj);
         }
-        float avx = __ldg(in + VX * P + co), avz = __ldg(in + VZ * P + co);
-        if (in_domain(g, R, gi, gj)) {
-            float dx = __ldg(a.dampx + gj + XO), dz = __ldg(a.dampz + gi + ZO);
-            float sx = dbwd<R>(s_atx, is, 1, a.k.cx) + dbwd<R>(s_atz, is, 1, a.k.cx) + dbwd<R>(s_atxz, is, W, a.k.cz);
-            float sz = dfwd<R>(s_pvx, is, W, a.k.cz) + dfwd<R>(s_pvz, is, W, a.k.cz) + dfwd<R>(s_atxz, is, 1, a.k.cx);
-            avx = avx + (-dt) * ((2.f * dx + dz) * avx + sx);
-            avz = avz + (-dt) * ((dx + 2.f * dz) * avz + sz);
+        for (int e = tid; e < HT * (W / 4); e += NTHREADS) {
+            int r = e / (W / 4), q = e - r * (W / 4);
+            int gi = i0 - 2 * R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
+            const float4 b = ld4(a.mat + 2 * P, g, gi, gj);
+            const float4 vx = COH ? ld4c(in + VX * P, g, gi, gj) : ld4(in + VX * P, g, gi, gj);
+            const float4 vz = COH ? ld4c(in + VZ * P, g, gi, gj) : ld4(in + VZ * P, g, gi, gj);
+            st4s(s_pvx + o, make_float4(vx.x * b.x, vx.y * b.y, vx.z * b.z, vx.w * b.w));
+            st4s(s_pvz + o, make_float4(vz.x * b.x, vz.y * b.y, vz.z * b.z, vz.w * b.w));
         }
-        if (!(gi < glo || gi > g.tnz - R - a.npml || gj < glo || gj > g.tnx - R - a.npml)) {
-        const long long sz_ = g.pitch;
-        // the new adjoint stresses this CTA wrote above (plain loads: written in this kernel)
-        const float atx = out[TXX * P + co], atz = out[TZZ * P + co], atxz = out[TXZ * P + co];
-        float dzp_vx, dxm_vz, dxp_vx, dzm_vz, dzp_tz, dxm_tx, dxp_txz, dzm_txz;
-        float vx = 0.f, vz = 0.f, tx = 0.f, tz = 0.f, txz = 0.f;
-        if (F) {
-            // DzpVx is formed from vz, as the reference does (elastic.cl:485)
-            dzp_vx = wfwd<R>(wvz, a.k.cz);
-            dxm_vz = gbwd<R>(F + VZ * P, co, 1, a.k.cx);
-            dxp_vx = gfwd<R>(F + VX * P, co, 1, a.k.cx);
-            dzm_vz = wbwd<R>(wvz, a.k.cz);
-            dzp_tz = wfwd<R>(wtz, a.k.cz);
-            dxm_tx = gbwd<R>(F + TXX * P, co, 1, a.k.cx);
-            dxp_txz = gfwd<R>(F + TXZ * P, co, 1, a.k.cx);
-            dzm_txz = wbwd<R>(wtxz, a.k.cz);
-            if (ENERGY) {
-                vx = F[VX * P + co];
-                vz = wvz[R];
-                tx = F[TXX * P + co];
-                tz = wtz[R];
-                txz = wtxz[R];
+        cp_wait_all();
+        __syncthreads();
+
+        // adjoint stresses on the tile plus an R-cell ring (Adj_update_tau); the
+        // tile's own cells go straight to the output
+        for (int e = tid; e < HV * VW; e += NTHREADS) {
+            int r = e / VW, cc = e - r * VW;
+            int gi = i0 - R + r, gj = j0 - R + cc;
+            int is = r * W + cc + R, iv = is + R * W;
+            const bool tile = r >= R && r < R + TZ && cc >= R && cc < R + TX && gi < g.tnz && gj < g.tnx;
+            float atx = s_atx[is], atz = s_atz[is], atxz = s_atxz[is];
+            if (in_domain(g, R, gi, gj)) {
+                float dx = __ldg(a.dampx + gj + XO), dz = __ldg(a.dampz + gi + ZO);
+                atx = atx + (-dt) * (dx * atx + dfwd<R>(s_pvx, iv, 1, a.k.cx));
+                atz = atz + (-dt) * (dz * atz + dbwd<R>(s_pvz, iv, W, a.k.cz));
+                atxz = atxz + (-dt) * ((dx + dz) * atxz + (dfwd<R>(s_pvx, iv, W, a.k.cz) + dbwd<R>(s_pvz, iv, 1, a.k.cx)));
+                s_atx[is] = atx;
+                s_atz[is] = atz;
+                s_atxz[is] = atxz;
             }
-        } else {
-#define B16F(f, k) bf(F16 + (f) * P, (k))
+            if (tile) {
+                const long long co = cell_off(g, gi, gj);
+                out[TXX * P + co] = atx;
+                out[TZZ * P + co] = atz;
+                out[TXZ * P + co] = atxz;
+            }
+        }
+        __syncthreads();
+
+        // material products of the new adjoint stresses
+        for (int e = tid; e < HV * VW; e += NTHREADS) {
+            int r = e / VW, cc = e - r * VW;
+            int gi = i0 - R + r, gj = j0 - R + cc;
+            int is = r * W + cc + R;
+            // lam = mu = 0 in the zero frame and beyond the allocated rows / columns
+            const bool alloc = gi + ZO >= 0 && gi + ZO < g.rows && gj + XO >= 0 && gj + XO < g.pitch;
+            const long long co = alloc ? cell_off(g, gi, gj) : 0;
+            const float lam = alloc ? __ldg(a.mat + co) : 0.f, mu = alloc ? __ldg(a.mat + P + co) : 0.f;
+            const float l2m = lam + 2.f * mu;
+            const float atx = s_atx[is], atz = s_atz[is], atxz = s_atxz[is];
+            s_atx[is] = l2m * atx;
+            s_atz[is] = lam * atz;
+            s_atxz[is] = mu * atxz;
+            s_pvx[is] = lam * atx;
+            s_pvz[is] = l2m * atz;
+        }
+        __syncthreads();
+
+        // adjoint velocities on the tile (Adj_update_v) and imaging (Grad)
+        if (gj >= g.tnx) continue;
+        // the imaged forward state: FP32, or (NARROW) BF16 / 24-bit snapshots
+        const float *F = !NARROW && av.fwd ? av.fwd + slot * a.fwd_stride : nullptr;
+        const __nv_bfloat16 *F16 = NARROW ? av.fwd16 + slot * a.fwd_stride : nullptr;
+        const unsigned char *F8 = NARROW && av.fwd8 ? av.fwd8 + slot * a.fwd_stride : nullptr;
+        const long long pz = g.pitch;
+        float wvz[2 * R + 1], wtz[2 * R + 1], wtxz[2 * R + 1];
+        const bool win = !NARROW && F && col_img && i0 + r0 + NK - 1 >= glo && i0 + r0 <= g.tnz - R - a.npml;
+        if (win) {
+            const long long c0 = cell_off(g, i0 + r0, gj);
+#pragma unroll
+            for (int m = 0; m < 2 * R; ++m) {
+                const long long o = c0 + (m - R) * pz;
+                wvz[m + 1] = __ldg(F + VZ * P + o);
+                wtz[m + 1] = __ldg(F + TZZ * P + o);
+                wtxz[m + 1] = __ldg(F + TXZ * P + o);
+            }
+        }
+        for (int k = 0; k < NK; ++k) {
+            const int r = r0 + k, gi = i0 + r;
+            if (gi >= g.tnz) break;
+            int is = (r + R) * W + c + 2 * R;
+            long long co = cell_off(g, gi, gj);
+            if (win) {  // the window moves to rows gi-R .. gi+R
+                const long long o = co + R * pz;
+                shift(wvz, __ldg(F + VZ * P + o));
+                shift(wtz, __ldg(F + TZZ * P + o));
+                shift(wtxz, __ldg(F + TXZ * P + o));
+            }
+            float avx = COH ? __ldcg(in + VX * P + co) : __ldg(in + VX * P + co);
+            float avz = COH ? __ldcg(in + VZ * P + co) : __ldg(in + VZ * P + co);
+            if (in_domain(g, R, gi, gj)) {
+                float dx = __ldg(a.dampx + gj + XO), dz = __ldg(a.dampz + gi + ZO);
+                float sx = dbwd<R>(s_atx, is, 1, a.k.cx) + dbwd<R>(s_atz, is, 1, a.k.cx) + dbwd<R>(s_atxz, is, W, a.k.cz);
+                float sz = dfwd<R>(s_pvx, is, W, a.k.cz) + dfwd<R>(s_pvz, is, W, a.k.cz) + dfwd<R>(s_atxz, is, 1, a.k.cx);
+                avx = avx + (-dt) * ((2.f * dx + dz) * avx + sx);
+                avz = avz + (-dt) * ((dx + 2.f * dz) * avz + sz);
+            }
+            if (col_img && gi >= glo && gi <= g.tnz - R - a.npml) {
+                const long long sz_ = g.pitch;
+                // the new adjoint stresses this CTA wrote above (plain loads: written in this kernel)
+                const float atx = out[TXX * P + co], atz = out[TZZ * P + co], atxz = out[TXZ * P + co];
+                float dzp_vx, dxm_vz, dxp_vx, dzm_vz, dzp_tz, dxm_tx, dxp_txz, dzm_txz;
+                float vx = 0.f, vz = 0.f, tx = 0.f, tz = 0.f, txz = 0.f;
+                if (!NARROW) {
+                    // DzpVx is formed from vz, as the reference does (elastic.cl:485)
+                    dzp_vx = wfwd<R>(wvz, a.k.cz);
+                    dxm_vz = gbwd<R>(F + VZ * P, co, 1, a.k.cx);
+                    dxp_vx = gfwd<R>(F + VX * P, co, 1, a.k.cx);
+                    dzm_vz = wbwd<R>(wvz, a.k.cz);
+                    dzp_tz = wfwd<R>(wtz, a.k.cz);
+                    dxm_tx = gbwd<R>(F + TXX * P, co, 1, a.k.cx);
+                    dxp_txz = gfwd<R>(F + TXZ * P, co, 1, a.k.cx);
+                    dzm_txz = wbwd<R>(wtxz, a.k.cz);
+                    if (ENERGY) {
+                        vx = F[VX * P + co];
+                        vz = wvz[R];
+                        tx = F[TXX * P + co];
+                        tz = wtz[R];
+                        txz = wtxz[R];
+                    }
+                } else {
+#define B16F(f, k) snapv(F16, F8, (f) * P + (k))
 #define BFWD(f, s)                                                                                       \
     (a.k.c##s[0] * (B16F(f, co + st) - B16F(f, co)) + a.k.c##s[1] * (B16F(f, co + 2 * st) - B16F(f, co - st)) + \
      (R == 4 ? a.k.c##s[2] * (B16F(f, co + 3 * st) - B16F(f, co - 2 * st)) +                              \
@@ -985,50 +1113,83 @@ __global__ void __launch_bounds__(NTHREADS, (R == 2 && !ENERGY) ? 6 : 1) adj_ste
      (R == 4 ? a.k.c##s[2] * (B16F(f, co + 2 * st) - B16F(f, co - 3 * st)) +                              \
                    a.k.c##s[3] * (B16F(f, co + 3 * st) - B16F(f, co - 4 * st))                            \
              : 0.f))
-            long long st = sz_;
-            dzp_vx = BFWD(VZ, z);
-            dzm_vz = BBWD(VZ, z);
-            dzp_tz = BFWD(TZZ, z);
-            dzm_txz = BBWD(TXZ, z);
-            st = 1;
-            dxm_vz = BBWD(VZ, x);
-            dxp_vx = BFWD(VX, x);
-            dxm_tx = BBWD(TXX, x);
-            dxp_txz = BFWD(TXZ, x);
-            if (ENERGY) {
-                vx = B16F(VX, co);
-                vz = B16F(VZ, co);
-                tx = B16F(TXX, co);
-                tz = B16F(TZZ, co);
-                txz = B16F(TXZ, co);
-            }
+                    long long st = sz_;
+                    dzp_vx = BFWD(VZ, z);
+                    dzm_vz = BBWD(VZ, z);
+                    dzp_tz = BFWD(TZZ, z);
+                    dzm_txz = BBWD(TXZ, z);
+                    st = 1;
+                    dxm_vz = BBWD(VZ, x);
+                    dxp_vx = BFWD(VX, x);
+                    dxm_tx = BBWD(TXX, x);
+                    dxp_txz = BFWD(TXZ, x);
+                    if (ENERGY) {
+                        vx = B16F(VX, co);
+                        vz = B16F(VZ, co);
+                        tx = B16F(TXX, co);
+                        tz = B16F(TZZ, co);
+                        txz = B16F(TXZ, co);
+                    }
 #undef B16F
 #undef BFWD
 #undef BBWD
+                }
+                const float b = __ldg(a.mat + 2 * P + co);
+                float img[NACC];
+                if (NS == 1) {  // one shot: read-modify-write in memory, as each step of the reference's Grad
+#pragma unroll
+                    for (int f = 0; f < NACC; ++f) img[f] = COH ? __ldcg(G + f * P + co) : G[f * P + co];
+                } else {
+#pragma unroll
+                    for (int f = 0; f < NACC; ++f) img[f] = s_acc[(f * TZ + r) * TX + c];
+                }
+                img[0] += 2.f * dt * (atx * dxp_vx + atz * dzm_vz) + dt * atxz * (dzp_vx + dxm_vz);
+                img[1] += dt * (atx + atz) * (dxp_vx + dzm_vz);
+                img[2] += -(dt * (b * b)) * (avx * (dxm_tx + dzm_txz) + avz * (dzp_tz + dxp_txz));
+                if (ENERGY) {
+                    float dt2 = dt * dt;
+                    img[3 % NACC] += 4.f * dt2 * (tx * tx * dxp_vx * dxp_vx + tz * tz * dzm_vz * dzm_vz) +
+                                     dt2 * txz * txz * (dzp_vx * dzp_vx + dxm_vz * dxm_vz);
+                    img[4 % NACC] += dt2 * (tx * tx + tz * tz) * (dxp_vx * dxp_vx + dzm_vz * dzm_vz);
+                    img[5 % NACC] += dt2 * (vx * vx * (dxm_tx * dxm_tx + dzm_txz * dzm_txz) +
+                                            vz * vz * (dzp_tz * dzp_tz + dxp_txz * dxp_txz));
+                }
+                if (NS == 1) {
+#pragma unroll
+                    for (int f = 0; f < NACC; ++f) G[f * P + co] = img[f];
+                } else {
+#pragma unroll
+                    for (int f = 0; f < NACC; ++f) s_acc[(f * TZ + r) * TX + c] = img[f];
+                }
+            }
+            // the residual the next step injects (Adj_injSrc, elastic_surface.cl:48-71),
+            // added to this step's output after the imaging has read it
+            if (av.epi_row >= 0) inject_epilogue(a, av.epi_row, slot, gi, gj, co, avx, avz, out);
+            out[VX * P + co] = avx;
+            out[VZ * P + co] = avz;
         }
-        const float b = __ldg(a.mat + 2 * P + co);
-        float gmu = G[0 * P + co], glam = G[1 * P + co], grho = G[2 * P + co];
-        gmu += 2.f * dt * (atx * dxp_vx + atz * dzm_vz) + dt * atxz * (dzp_vx + dxm_vz);
-        glam += dt * (atx + atz) * (dxp_vx + dzm_vz);
-        grho += -(dt * (b * b)) * (avx * (dxm_tx + dzm_txz) + avz * (dzp_tz + dxp_txz));
-        G[0 * P + co] = gmu;
-        G[1 * P + co] = glam;
-        G[2 * P + co] = grho;
-        if (ENERGY) {
-            float dt2 = dt * dt;
-            G[3 * P + co] += 4.f * dt2 * (tx * tx * dxp_vx * dxp_vx + tz * tz * dzm_vz * dzm_vz) +
-                             dt2 * txz * txz * (dzp_vx * dzp_vx + dxm_vz * dxm_vz);
-            G[4 * P + co] += dt2 * (tx * tx + tz * tz) * (dxp_vx * dxp_vx + dzm_vz * dzm_vz);
-            G[5 * P + co] += dt2 * (vx * vx * (dxm_tx * dxm_tx + dzm_txz * dzm_txz) +
-                                    vz * vz * (dzp_tz * dzp_tz + dxp_txz * dxp_txz));
-        }
-        }
-        // the residual the next step injects (Adj_injSrc, elastic_surface.cl:48-71),
-        // added to this step's output after the imaging has read it
-        if (a.epi_row >= 0) inject_epilogue(a, slot, gi, gj, co, avx, avz, out);
-        out[VX * P + co] = avx;
-        out[VZ * P + co] = avz;
     }
+    if (NS > 1) {
+        for (int k = 0; k < NK; ++k) {
+            const int gi = i0 + r0 + k;
+            if (col_img && gi >= glo && gi <= g.tnz - R - a.npml) {
+                const long long co = cell_off(g, gi, gj);
+#pragma unroll
+                for (int f = 0; f < NACC; ++f) G[f * P + co] = s_acc[(f * TZ + r0 + k) * TX + c];
+            }
+        }
+    }
+}
+
+// NARROW: the imaging reads BF16 or 24-bit snapshots (fwd16, fwd8) instead
+// of FP32 states.
+template <int R, int TZ, bool ENERGY, int NS, bool NARROW>
+__global__ void __launch_bounds__(NTHREADS, AdjOccupancy<R, ENERGY, NS>::value)
+    adj_step(const __grid_constant__ AdjArgs a)
+{
+    extern __shared__ float4 smem4[];
+    adj_tile<R, TZ, ENERGY, NS, NARROW, false>(a, a, blockIdx.x, blockIdx.y, blockIdx.z,
+                                               reinterpret_cast<float *>(smem4));
 }
 
 // ---------------------------------------------------------------------------
@@ -1058,10 +1219,12 @@ struct ExactArgs {
     long long in_stride, out_stride;
     const float *s1, *s0;   // forward states S_{t+1}, S_t, slot 0 (FP32)
     long long s1_stride, s0_stride;
-    // BF16 snapshots instead (kernel instance BF): S_{t+1} always, S_t when
-    // s0h is set (else S_t is the FP32 restart state s0, rounded to BF16 as
-    // it is read)
+    // BF16 or 24-bit snapshots instead (kernel instance BF): S_{t+1} always,
+    // S_t when s0h is set (else S_t is the FP32 restart state s0, rounded to
+    // the snapshot format as it is read); s1b / s0b: the byte planes of
+    // 24-bit snapshots (NULL for BF16)
     const __nv_bfloat16 *s1h, *s0h;
+    const unsigned char *s1b, *s0b;
     const float *mat;       // lam, mu, b, rho planes
     const float *dampx, *dampz;
     float *gacc;            // [slot][3][plane]: Glam, Gmu, Gb
@@ -1111,6 +1274,9 @@ __global__ void __launch_bounds__(NTHREADS) exact_adj_step(const __grid_constant
     const float *S0 = (BF && a.s0h) ? nullptr : a.s0 + slot * a.s0_stride;
     const __nv_bfloat16 *H1 = BF ? a.s1h + slot * a.s1_stride : nullptr;
     const __nv_bfloat16 *H0 = (BF && a.s0h) ? a.s0h + slot * a.s0_stride : nullptr;
+    const unsigned char *B1 = (BF && a.s1b) ? a.s1b + slot * a.s1_stride : nullptr;
+    const unsigned char *B0 = (BF && a.s0b) ? a.s0b + slot * a.s0_stride : nullptr;
+    const bool x24 = a.s1b != nullptr;  // 24-bit snapshots
     float *G = a.gacc + slot * a.gacc_stride;
     const float dt = a.k.dt;
 
@@ -1191,21 +1357,24 @@ __global__ void __launch_bounds__(NTHREADS) exact_adj_step(const __grid_constant
         auto f32 = [&](const float *S) {
             return [=](int f) { return [=](long long i) { return __ldg(S + f * P + i); }; };
         };
-        auto b16 = [&](const __nv_bfloat16 *S) {
-            return [=](int f) { return [=](long long i) { return ldh(S + f * P, i); }; };
+        auto snap = [&](const __nv_bfloat16 *S, const unsigned char *B) {
+            return [=](int f) { return [=](long long i) { return snapv(S, B, f * P + i); }; };
         };
-        auto f32_as_b16 = [&](const float *S) {
+        auto f32_as_snap = [&](const float *S) {
             return [=](int f) {
-                return [=](long long i) { return __bfloat162float(__float2bfloat16_rn(__ldg(S + f * P + i))); };
+                return [=](long long i) {
+                    const float v = __ldg(S + f * P + i);
+                    return x24 ? fp24_round(v) : __bfloat162float(__float2bfloat16_rn(v));
+                };
             };
         };
         float dxp_vx, dzm_vz, dxm_vz, dzp_vx, dxm_tx, dzm_txz, dzp_tz, dxp_txz;
         if (BF) {
-            vdiffs(b16(H1), dxp_vx, dzm_vz, dxm_vz, dzp_vx);
+            vdiffs(snap(H1, B1), dxp_vx, dzm_vz, dxm_vz, dzp_vx);
             if (H0)
-                sdiffs(b16(H0), dxm_tx, dzm_txz, dzp_tz, dxp_txz);
+                sdiffs(snap(H0, B0), dxm_tx, dzm_txz, dzp_tz, dxp_txz);
             else
-                sdiffs(f32_as_b16(S0), dxm_tx, dzm_txz, dzp_tz, dxp_txz);
+                sdiffs(f32_as_snap(S0), dxm_tx, dzm_txz, dzp_tz, dxp_txz);
         } else {
             vdiffs(f32(S1), dxp_vx, dzm_vz, dxm_vz, dzp_vx);
             sdiffs(f32(S0), dxm_tx, dzm_txz, dzp_tz, dxp_txz);

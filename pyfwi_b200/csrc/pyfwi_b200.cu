@@ -7,6 +7,7 @@
 // all enqueued on the caller's stream (optionally replayed as a CUDA graph).
 #include "pyfwi_b200.h"
 #include "kernels.cuh"
+#include "persist_kernels.cuh"
 #include "stream_kernels.cuh"
 
 #include <nvtx3/nvToolsExt.h>
@@ -61,13 +62,17 @@ constexpr size_t ALIGN = 256;
 size_t up(size_t x, size_t a = ALIGN) { return (x + a - 1) / a * a; }
 
 // kernel variants: 0..2 tile kernels with 16 / 8 / 32 rows per tile,
-// 3..5 streaming kernels whose CTAs span 128 / 64 / 256 columns
-constexpr int TILE_TZ[] = {16, 8, 32, 0, 0, 0};
-constexpr int STREAM_W[] = {0, 0, 0, 128, 64, 256};
-constexpr int N_TILES = 6;
+// 3..5 streaming kernels whose CTAs span 128 / 64 / 256 columns, 6..7 the
+// 16-row tile kernels whose adjoint CTAs carry 2 / 4 shots each (the
+// forward step of 6..7 is variant 0's)
+constexpr int TILE_TZ[] = {16, 8, 32, 0, 0, 0, 16, 16};
+constexpr int STREAM_W[] = {0, 0, 0, 128, 64, 256, 0, 0};
+constexpr int ADJ_NS[] = {1, 1, 1, 1, 1, 1, 2, 4};
+constexpr int N_TILES = 8;
 constexpr int FWD_PF = 4, ADJ_PF = 2;  // rows the streaming kernels fetch ahead
 constexpr size_t ERR_OFF = 128;         // byte offset of the device error word in the header
 constexpr size_t CHECK_OFF = 192;       // byte offset of the frame-check counter (uint64) in the header
+constexpr size_t BAR_OFF = 224;         // byte offset of the persistent kernels' grid barrier (2 x uint32)
 
 // cuTensorMapEncodeTiled, resolved through the runtime so the library does
 // not link the driver API directly
@@ -89,11 +94,13 @@ struct pyfwi_plan {
     Grid g;
     Coef k;
     Lines lines;
-    int R, tz, st_w, atz, ast_w, chunk_opt, nacc, G, ngroups, seg, M, n_inj;  // a*: adjoint step variant
+    int R, tz, st_w, atz, ast_w, ans, chunk_opt, nacc, G, ngroups, seg, M, n_inj;  // a*: adjoint step variant
     bool exact_adj = false;  // PYFWI_ADJOINT_EXACT
+    bool persist = false;    // time loops as persistent kernels (options.persist, where the layout allows)
+    int fwd_cap = 0, adj_cap = 0;  // co-resident CTAs of the persistent kernels on this device
     long long state;  // floats per state (5 planes)
     // workspace offsets in bytes
-    size_t o_hdr, o_src, o_red, o_mat, o_dampx, o_dampz, o_work, o_adj, o_gacc, o_store, o_store16, total;
+    size_t o_hdr, o_src, o_red, o_mat, o_dampx, o_dampz, o_work, o_adj, o_gacc, o_store, o_store16, o_store8, total;
     long long launches = 0;
     bool model_set = false, fwd_valid = false;
     // per-kernel event timing (pyfwi_profile_enable)
@@ -162,10 +169,14 @@ int launch_fwd(pyfwi_plan *p, const StepArgs &a, int nslots, cudaStream_t s, boo
         size_t sm = FwdShape<R, TZ>::FLOATS * sizeof(float);
         static bool attr = false;
         if (!attr) {
-            CK(cudaFuncSetAttribute(fwd_step<R, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            CK(cudaFuncSetAttribute(fwd_step<R, TZ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            CK(cudaFuncSetAttribute(fwd_step<R, TZ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
             attr = true;
         }
-        fwd_step<R, TZ><<<grid, NTHREADS, sm, s>>>(a);
+        if (a.snap8)  // 24-bit snapshots written by their own instance (keeps the others' registers)
+            fwd_step<R, TZ, true><<<grid, NTHREADS, sm, s>>>(a);
+        else
+            fwd_step<R, TZ, false><<<grid, NTHREADS, sm, s>>>(a);
     } else {
         size_t sm = RevShape<R, TZ>::FLOATS * sizeof(float);
         static bool attr = false;
@@ -194,28 +205,104 @@ int launch_inject(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
     return PYFWI_OK;
 }
 
-template <int R, int TZ, bool E>
+template <int R, int TZ, bool E, int NS, bool NARROW>
 int launch_adj_t(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
 {
     int rc = launch_inject(p, a, nslots, s);
     if (rc) return rc;
-    dim3 grid((p->g.tnx + TX - 1) / TX, (p->g.tnz + TZ - 1) / TZ, nslots);
-    size_t sm = AdjShape<R, TZ>::FLOATS * sizeof(float);
+    dim3 grid((p->g.tnx + TX - 1) / TX, (p->g.tnz + TZ - 1) / TZ, (nslots + NS - 1) / NS);
+    size_t sm = adj_smem_floats<R, TZ, E, NS>() * sizeof(float);
     static bool attr = false;
     if (!attr) {
-        CK(cudaFuncSetAttribute(adj_step<R, TZ, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        CK(cudaFuncSetAttribute(adj_step<R, TZ, E, NS, NARROW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sm));
         attr = true;
     }
-    adj_step<R, TZ, E><<<grid, NTHREADS, sm, s>>>(a);
+    AdjArgs b = a;
+    b.nslots = nslots;
+    adj_step<R, TZ, E, NS, NARROW><<<grid, NTHREADS, sm, s>>>(b);
     p->launches++;
     CKL();
     return PYFWI_OK;
 }
 
+template <int R, int TZ, int NS>
+int launch_adj_ns(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
+{
+    return p->nacc == 6 ? launch_adj_t<R, TZ, true, NS, false>(p, a, nslots, s)
+                        : launch_adj_t<R, TZ, false, NS, false>(p, a, nslots, s);
+}
+
 template <int R, int TZ>
 int launch_adj(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
 {
-    return p->nacc == 6 ? launch_adj_t<R, TZ, true>(p, a, nslots, s) : launch_adj_t<R, TZ, false>(p, a, nslots, s);
+    if (a.fwd16) {  // BF16 / 24-bit snapshots: the 16-row kernel, one shot per CTA (the plan picks no other)
+        if (TZ != 16 || p->ans != 1) return fail(PYFWI_E_INVALID, "snapshots are imaged by adjoint variant 0 only");
+        return p->nacc == 6 ? launch_adj_t<R, 16, true, 1, true>(p, a, nslots, s)
+                            : launch_adj_t<R, 16, false, 1, true>(p, a, nslots, s);
+    }
+    if (TZ == 16 && p->ans == 2) return launch_adj_ns<R, TZ, 2>(p, a, nslots, s);
+    if (TZ == 16 && p->ans == 4) return launch_adj_ns<R, TZ, 4>(p, a, nslots, s);
+    return launch_adj_ns<R, TZ, 1>(p, a, nslots, s);
+}
+
+// ---- persistent kernels ----------------------------------------------------
+// Co-resident CTAs of `kern` with `smem` bytes of shared memory on the
+// current device (the most a cooperative launch may have).
+int coresident(const void *kern, size_t smem, int *out)
+{
+    int dev = 0, sms = 0, per = 0, coop = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    if (!coop) return fail(PYFWI_E_CUDA, "the device does not support cooperative launches");
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, NTHREADS, smem));
+    if (per < 1) return fail(PYFWI_E_CUDA, "a persistent kernel does not fit on an SM");
+    *out = per * sms;
+    return PYFWI_OK;
+}
+
+template <int R, int TZ>
+int launch_fwd_persist(pyfwi_plan *p, const FwdPersistArgs &a, cudaStream_t s)
+{
+    const size_t sm = FwdShape<R, TZ>::FLOATS * sizeof(float);
+    const void *kern = reinterpret_cast<const void *>(fwd_persist<R, TZ>);
+    if (!p->fwd_cap) {
+        CK(cudaFuncSetAttribute(fwd_persist<R, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        int rc = coresident(kern, sm, &p->fwd_cap);
+        if (rc) return rc;
+    }
+    const int nwork = a.ntx * a.ntz * a.nslots;
+    void *args[] = {const_cast<FwdPersistArgs *>(&a)};
+    CK(cudaLaunchCooperativeKernel(kern, dim3(std::min(nwork, p->fwd_cap)), dim3(NTHREADS), args, sm, s));
+    p->launches++;
+    return PYFWI_OK;
+}
+
+template <int R, int TZ, bool E>
+int launch_adj_persist_t(pyfwi_plan *p, const AdjPersistArgs &a, cudaStream_t s)
+{
+    const size_t sm = AdjShape<R, TZ>::FLOATS * sizeof(float);
+    const void *kern = reinterpret_cast<const void *>(adj_persist<R, TZ, E>);
+    if (!p->adj_cap) {
+        CK(cudaFuncSetAttribute(adj_persist<R, TZ, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        int rc = coresident(kern, sm, &p->adj_cap);
+        if (rc) return rc;
+    }
+    const int nwork = a.ntx * a.ntz * a.a.nslots;
+    void *args[] = {const_cast<AdjPersistArgs *>(&a)};
+    CK(cudaLaunchCooperativeKernel(kern, dim3(std::min(nwork, p->adj_cap)), dim3(NTHREADS), args, sm, s));
+    p->launches++;
+    return PYFWI_OK;
+}
+
+// Gradient accumulator slots the adjoint kernel writes for a launch of
+// `nslots` shots: one per CTA shot group of the tile kernel, one per shot
+// for the others.
+int acc_slots(const pyfwi_plan *p, int nslots)
+{
+    const int ns = (!p->exact_adj && !p->ast_w) ? p->ans : 1;
+    return (nslots + ns - 1) / ns;
 }
 
 // Event pair around one step launch when profiling (kind 0 fwd, 1 adj, 2 rev).
@@ -389,10 +476,15 @@ struct Buf {
     long long stride;  // floats between slots
 };
 
+// Snapshots narrower than FP32 (BF16, or 24 bits: a BF16 plane plus a byte
+// plane) hold the states of the segment being imaged.
 bool bf16_snaps(const pyfwi_plan *p)
 {
-    return p->opt.checkpoint == PYFWI_CKPT_EXACT && p->opt.snapshot == PYFWI_SNAP_BF16;
+    return p->opt.checkpoint == PYFWI_CKPT_EXACT &&
+           (p->opt.snapshot == PYFWI_SNAP_BF16 || p->opt.snapshot == PYFWI_SNAP_FP24);
 }
+
+bool fp24_snaps(const pyfwi_plan *p) { return bf16_snaps(p) && p->opt.snapshot == PYFWI_SNAP_FP24; }
 
 // exact mode, per slot of the store: M restart states S_0, S_seg, ...
 // S_{(M-1)seg}, then (FP32 snapshots) the seg states of the segment being
@@ -417,6 +509,12 @@ Buf exact_state(pyfwi_plan *p, void *ws, int s)
 __nv_bfloat16 *snap_at(pyfwi_plan *p, void *ws, int k)
 {
     return at<__nv_bfloat16>(ws, p->o_store16) + (long long)k * p->state;
+}
+
+// its byte planes (24-bit snapshots; NULL for BF16)
+unsigned char *snap8_at(pyfwi_plan *p, void *ws, int k)
+{
+    return fp24_snaps(p) ? at<unsigned char>(ws, p->o_store8) + (long long)k * p->state : nullptr;
 }
 
 StepArgs base_step(pyfwi_plan *p, void *ws)
@@ -445,11 +543,109 @@ float4 src_at(const pyfwi_plan *p, int inj)
     return make_float4(v[0], v[1], v[2], v[3]);
 }
 
+// The persistent kernels run this call's time loops: the plan allows them
+// and the stream is not being captured by the caller (cooperative launches
+// stay out of the caller's graphs).
+bool use_persist(const pyfwi_plan *p, cudaStream_t st)
+{
+    if (!p->persist) return false;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone;
+}
+
+unsigned *barrier_words(void *ws) { return at<unsigned>(ws, BAR_OFF); }
+
+// The forward pass of a group as persistent launches of up to
+// PERSIST_CHUNK steps (layout: every step stored in FP32, M == 1).
+int persist_pass(pyfwi_plan *p, void *ws, int s0, int n, float *traces, cudaStream_t st)
+{
+    const pyfwi_geometry &G = p->geom;
+    StepArgs a = base_step(p, ws);
+    a.shot0 = s0;
+    a.traces = traces;
+    FwdPersistArgs pa;
+    memset(&pa, 0, sizeof pa);
+    pa.a = a;
+    pa.store = at<float>(ws, p->o_store);
+    pa.sstride = store_stride(p);
+    pa.state = p->state;
+    pa.dt_scale = G.dt_scale;
+    pa.nt_ext = G.nt_ext;
+    pa.record = traces != nullptr;
+    pa.nslots = n;
+    pa.ntx = (p->g.tnx + TX - 1) / TX;
+    pa.ntz = (p->g.tnz + p->tz - 1) / p->tz;
+    pa.bar = barrier_words(ws);
+    pa.err = at<int>(ws, ERR_OFF);
+    pa.limit_ns = BARRIER_WAIT_NS;
+    for (int t0 = 0; t0 < G.nt; t0 += PERSIST_CHUNK) {
+        pa.t0 = t0;
+        pa.t1 = std::min(t0 + PERSIST_CHUNK, G.nt);
+        pa.k0 = t0 / G.dt_scale;
+        pa.nk = (pa.t1 - 1) / G.dt_scale - pa.k0 + 1;
+        for (int q = 0; q < pa.nk; ++q) pa.wav[q] = src_at(p, pa.k0 + q);
+        CK(cudaMemsetAsync(pa.bar, 0, 2 * sizeof(unsigned), st));
+        ProfileScope prof(p, st, 0, n * (pa.t1 - t0));
+        int rc = PYFWI_E_INVALID;
+#define CASE(R_, TZ_) \
+    if (p->R == R_ && p->tz == TZ_) rc = launch_fwd_persist<R_, TZ_>(p, pa, st);
+        CASE(2, 16) CASE(2, 8) CASE(2, 32) CASE(4, 16) CASE(4, 8) CASE(4, 32)
+#undef CASE
+        if (rc) return rc;
+    }
+    return PYFWI_OK;
+}
+
+int inj_row_of(const pyfwi_plan *p, int t);
+
+// The adjoint steps nt-1 .. 1 of a group as one persistent launch (the first
+// step's residual is injected by its own launch, as in adjoint_iter).
+int persist_backward(pyfwi_plan *p, void *ws, AdjArgs &a, int n, cudaStream_t st)
+{
+    const pyfwi_geometry &G = p->geom;
+    float *adj = at<float>(ws, p->o_adj);
+    a.nslots = n;
+    a.in = adj;
+    a.in_stride = a.out_stride = 2 * p->state;
+    a.inj_row = inj_row_of(p, G.nt - 1);
+    int rc = launch_inject(p, a, n, st);
+    if (rc) return rc;
+    if (G.nt < 2) return PYFWI_OK;
+    AdjPersistArgs pa;
+    memset(&pa, 0, sizeof pa);
+    pa.a = a;
+    pa.adj = adj;
+    pa.store = at<float>(ws, p->o_store);
+    pa.sstride = store_stride(p);
+    pa.state = p->state;
+    pa.t_hi = G.nt;
+    pa.t_lo = 1;
+    pa.ping0 = 0;
+    pa.nt = G.nt;
+    pa.nt_ext = G.nt_ext;
+    pa.dt_scale = G.dt_scale;
+    pa.ntx = (p->g.tnx + TX - 1) / TX;
+    pa.ntz = (p->g.tnz + p->atz - 1) / p->atz;
+    pa.bar = barrier_words(ws);
+    pa.err = at<int>(ws, ERR_OFF);
+    pa.limit_ns = BARRIER_WAIT_NS;
+    CK(cudaMemsetAsync(pa.bar, 0, 2 * sizeof(unsigned), st));
+    ProfileScope prof(p, st, 1, n * (G.nt - 1));
+    rc = PYFWI_E_INVALID;
+#define CASE(R_, TZ_)                                                                                          \
+    if (p->R == R_ && p->atz == TZ_)                                                                           \
+        rc = p->nacc == 6 ? launch_adj_persist_t<R_, TZ_, true>(p, pa, st) : launch_adj_persist_t<R_, TZ_, false>(p, pa, st);
+    CASE(2, 16) CASE(2, 8) CASE(2, 32) CASE(4, 16) CASE(4, 8) CASE(4, 32)
+#undef CASE
+    return rc;
+}
+
 // One forward pass of a group (exact mode), optionally recording traces.
 int exact_pass(pyfwi_plan *p, void *ws, int s0, int n, float *traces, cudaStream_t st)
 {
     Buf z = exact_state(p, ws, 0);
     for (int q = 0; q < n; ++q) CK(cudaMemsetAsync(z.base + q * z.stride, 0, p->state * sizeof(float), st));
+    if (use_persist(p, st)) return persist_pass(p, ws, s0, n, traces, st);
     StepArgs a = base_step(p, ws);
     a.shot0 = s0;
     a.traces = traces;
@@ -466,6 +662,7 @@ int exact_pass(pyfwi_plan *p, void *ws, int s0, int n, float *traces, cudaStream
         a.rec_row = (inj && traces && k < p->geom.nt_ext) ? k : -1;
         const int last_lo = (p->M - 1) * p->seg;
         a.snap = bf16_snaps(p) && t >= last_lo ? snap_at(p, ws, t - last_lo) : nullptr;
+        a.snap8 = a.snap ? snap8_at(p, ws, t - last_lo) : nullptr;
         a.snap_stride = (long long)p->seg * p->state;
         int rc = step_fwd(p, a, n, st, false, at<float>(ws, 0));
         if (rc) return rc;
@@ -626,6 +823,7 @@ int exact_backward(pyfwi_plan *p, void *ws, const float *const *residual, int s0
                     out = work_state(p, ws, (t + 1) & 1);
                     if (t > t_lo) in = work_state(p, ws, t & 1);
                     f.snap = snap_at(p, ws, t - t_lo);
+                    f.snap8 = snap8_at(p, ws, t - t_lo);
                     f.snap_stride = (long long)p->seg * p->state;
                 } else {
                     out = {store + (long long)(p->M + t - t_lo) * p->state, sstride};
@@ -646,8 +844,10 @@ int exact_backward(pyfwi_plan *p, void *ws, const float *const *residual, int s0
             if (bf16_snaps(p)) {
                 // snapshot k holds S_{t_lo+k+1}; S_{t_lo} is the FP32 restart state
                 e.s1h = snap_at(p, ws, t - t_lo);
+                e.s1b = snap8_at(p, ws, t - t_lo);
                 e.s1_stride = (long long)p->seg * p->state;
                 e.s0h = t > t_lo ? snap_at(p, ws, t - t_lo - 1) : nullptr;
+                e.s0b = t > t_lo ? snap8_at(p, ws, t - t_lo - 1) : nullptr;
                 Buf s_t = exact_state(p, ws, t_lo);
                 e.s0 = t > t_lo ? nullptr : s_t.base;
                 e.s0_stride = t > t_lo ? e.s1_stride : s_t.stride;
@@ -759,6 +959,9 @@ int gradient_enqueue(pyfwi_plan *p, void *ws, const float *const *residual, int3
             const float *zero[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
             rc = exact_backward(p, ws, residual ? residual : zero, s0, n, st);
             if (rc) return rc;
+        } else if (p->opt.checkpoint == PYFWI_CKPT_EXACT && use_persist(p, st)) {
+            rc = persist_backward(p, ws, a, n, st);  // M == 1: every step stored
+            if (rc) return rc;
         } else if (p->opt.checkpoint == PYFWI_CKPT_EXACT) {
             StepArgs f = base_step(p, ws);
             f.shot0 = s0;
@@ -772,6 +975,7 @@ int gradient_enqueue(pyfwi_plan *p, void *ws, const float *const *residual, int3
                             out = work_state(p, ws, (t + 1) & 1);
                             if (t > t_lo) in = work_state(p, ws, t & 1);
                             f.snap = snap_at(p, ws, t - t_lo);
+                            f.snap8 = snap8_at(p, ws, t - t_lo);
                             f.snap_stride = (long long)p->seg * p->state;
                         } else {
                             out = {at<float>(ws, p->o_store) + (long long)(p->M + t - t_lo) * p->state,
@@ -798,6 +1002,7 @@ int gradient_enqueue(pyfwi_plan *p, void *ws, const float *const *residual, int3
                     if (bf16_snaps(p)) {
                         a.fwd = nullptr;
                         a.fwd16 = snap_at(p, ws, t - t_lo);
+                        a.fwd8 = snap8_at(p, ws, t - t_lo);
                         a.fwd_stride = (long long)p->seg * p->state;
                     } else {
                         a.fwd = at<float>(ws, p->o_store) + (long long)(p->M + t - t_lo) * p->state;
@@ -840,8 +1045,8 @@ int gradient_enqueue(pyfwi_plan *p, void *ws, const float *const *residual, int3
     }
 
     const long long nplane = (long long)p->nacc * p->g.plane;
-    if (p->G > 1) {
-        reduce_slots_kernel<<<grid_blocks(nplane), 256, 0, st>>>(gacc, nplane, p->G, nplane);
+    if (acc_slots(p, p->G) > 1) {
+        reduce_slots_kernel<<<grid_blocks(nplane), 256, 0, st>>>(gacc, nplane, acc_slots(p, p->G), nplane);
         p->launches++;
         CKL();
     }
@@ -984,10 +1189,10 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
                 return fail(PYFWI_E_INVALID, "checkpoint steps must be increasing and inside [0, nt)");
         if (opt->chp[opt->nchp - 1] != G.nt - 1) return fail(PYFWI_E_INVALID, "last checkpoint must be step nt-1");
     }
-    if (opt->snapshot != PYFWI_SNAP_FP32 && opt->snapshot != PYFWI_SNAP_BF16)
+    if (opt->snapshot != PYFWI_SNAP_FP32 && opt->snapshot != PYFWI_SNAP_BF16 && opt->snapshot != PYFWI_SNAP_FP24)
         return fail(PYFWI_E_INVALID, "unknown snapshot format");
-    if (opt->snapshot == PYFWI_SNAP_BF16 && opt->checkpoint != PYFWI_CKPT_EXACT)
-        return fail(PYFWI_E_INVALID, "bf16 snapshots need the exact checkpoint mode");
+    if (opt->snapshot != PYFWI_SNAP_FP32 && opt->checkpoint != PYFWI_CKPT_EXACT)
+        return fail(PYFWI_E_INVALID, "bf16 and 24-bit snapshots need the exact checkpoint mode");
     if (opt->tile < 0 || opt->tile >= N_TILES) return fail(PYFWI_E_INVALID, "tile variant out of range");
     if (opt->adj_tile < 0 || opt->adj_tile > N_TILES) return fail(PYFWI_E_INVALID, "adj_tile out of range");
     if (opt->adjoint != PYFWI_ADJOINT_REFERENCE && opt->adjoint != PYFWI_ADJOINT_EXACT)
@@ -1009,9 +1214,12 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
     const int av = opt->adj_tile ? opt->adj_tile - 1 : opt->tile;
     p->atz = TILE_TZ[av];
     p->ast_w = STREAM_W[av];
-    if (opt->snapshot == PYFWI_SNAP_BF16 && p->ast_w) {  // BF16 snapshots are read by the tile adjoint kernel
+    p->ans = ADJ_NS[av];
+    if (opt->snapshot != PYFWI_SNAP_FP32 && opt->checkpoint == PYFWI_CKPT_EXACT) {
+        // snapshots are read by the 16-row tile adjoint kernel with one shot per CTA
         p->ast_w = 0;
         p->atz = TILE_TZ[0];
+        p->ans = 1;
     }
     p->chunk_opt = opt->chunk;
     p->nacc = opt->energy ? 6 : 3;
@@ -1044,6 +1252,11 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
     p->seg = opt->segment > 0 && opt->segment < G.nt ? opt->segment : G.nt;
     p->M = (G.nt + p->seg - 1) / p->seg;
     p->n_inj = (G.nt + G.dt_scale - 1) / G.dt_scale;
+    // persistent time loops: every step stored in FP32 (one segment), tile
+    // kernels with one shot per adjoint CTA, the reference adjoint
+    p->persist = opt->persist && opt->checkpoint == PYFWI_CKPT_EXACT && p->M == 1 &&
+                 opt->snapshot == PYFWI_SNAP_FP32 && !p->exact_adj && !p->st_w && !p->ast_w && p->ans == 1;
+    if (p->persist) p->opt.graph = 0;  // a few launches per call: nothing to replay
 
     const size_t pf = (size_t)p->g.plane * sizeof(float), sb = (size_t)p->state * sizeof(float);
     // regions holding planes start on a row of the workspace (a multiple of
@@ -1083,6 +1296,8 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
     o = upr(o);
     p->o_store16 = o;
     if (bf16_snaps(p)) o += up((size_t)p->seg * p->state * sizeof(__nv_bfloat16) * p->G);
+    p->o_store8 = o;
+    if (fp24_snaps(p)) o += up((size_t)p->seg * p->state * p->G);
     p->total = o;
     *out = p;
     return PYFWI_OK;
@@ -1161,7 +1376,9 @@ int pyfwi_device_error(pyfwi_plan *p, void *ws, size_t bytes, int32_t *code, voi
     CK(cudaMemsetAsync(word, 0, sizeof v, st));
     CK(cudaStreamSynchronize(st));
     *code = v;
-    if (v) return fail(PYFWI_E_TIMEOUT, "device error word %d: a streaming kernel stopped early", v);
+    if (v)
+        return fail(PYFWI_E_TIMEOUT, "device error word %d: %s", v,
+                    v == 3 ? "a persistent kernel gave up at a grid barrier" : "a streaming kernel stopped early");
     return PYFWI_OK;
 }
 
@@ -1223,6 +1440,20 @@ int pyfwi_wait_selftest(pyfwi_plan *p, void *ws, size_t bytes, int64_t limit_ns,
     if (rc) return rc;
     wait_selftest_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(at<int>(ws, ERR_OFF),
                                                                           (unsigned long long)limit_ns);
+    CKL();
+    return PYFWI_OK;
+}
+
+int pyfwi_barrier_selftest(pyfwi_plan *p, void *ws, size_t bytes, int64_t limit_ns, void *stream)
+{
+    if (!p) return fail(PYFWI_E_INVALID, "NULL plan");
+    int rc = check_ws(p, ws, bytes);
+    if (rc) return rc;
+    if (limit_ns < 1000 || limit_ns > 10000000000LL) return fail(PYFWI_E_INVALID, "limit_ns out of range");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    CK(cudaMemsetAsync(barrier_words(ws), 0, 2 * sizeof(unsigned), st));
+    barrier_selftest_kernel<<<2, 32, 0, st>>>(barrier_words(ws), at<int>(ws, ERR_OFF), (unsigned long long)limit_ns);
+    p->launches++;
     CKL();
     return PYFWI_OK;
 }

@@ -15,7 +15,10 @@
 //     bytes needed;
 //   * the first call on each device looks the array's device address up
 //     (cudaGetSymbolAddress, with that device current); make that first call
-//     before any stream capture on the device;
+//     before any stream capture on the device.  The address is kept for the
+//     life of the process, so the entry point must not be used again after
+//     a cudaDeviceReset of that device (the module, and the array with it,
+//     would be loaded afresh at another address);
 //   * every call on a device reuses the same array and leaves its contents
 //     behind; the call clears what must start from zero itself.  Calls whose
 //     work overlaps on the GPU (other streams, other host threads) race on

@@ -371,8 +371,10 @@ __global__ void __launch_bounds__(W - 2 * R) fwd_stream(const __grid_constant__ 
             out[TXX * P + co] = txx;
             out[TZZ * P + co] = tzz;
             out[TXZ * P + co] = txz;
-            if (a.snap) write_snap(a.snap + slot * a.snap_stride, P, co, wvx[R], wvz[R], txx, tzz, txz);
-            if (a.rec_row >= 0) record_cell(a, in, shot, i, j);
+            if (a.snap)
+                write_snap(a.snap + slot * a.snap_stride, a.snap8 ? a.snap8 + slot * a.snap_stride : nullptr, P, co,
+                           wvx[R], wvz[R], txx, tzz, txz);
+            if (a.rec_row >= 0) record_cell(a, a.rec_row, in, shot, i, j);
         }
     }
     drain(bar, NB, kb, ke, PFW, s_abort, a.err);

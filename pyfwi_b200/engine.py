@@ -126,7 +126,8 @@ class Plan:
 
     def check_device(self):
         """Synchronise the device stream and raise NativeError if a streaming
-        kernel gave up waiting for a row copy since the last check."""
+        kernel gave up waiting for a row copy, or a persistent kernel at a
+        grid barrier, since the last check."""
         code = ctypes.c_int32()
         N.check(self.lib.pyfwi_device_error(self.handle, self.ws, self.ws_bytes, ctypes.byref(code),
                                             _stream(self.device)))
@@ -155,6 +156,13 @@ class Plan:
         up after limit_ns and sets the error word (read by check_device)."""
         N.check(self.lib.pyfwi_wait_selftest(self.handle, self.ws, self.ws_bytes, int(limit_ns),
                                              _stream(self.device)))
+
+    def barrier_selftest(self, limit_ns):
+        """pyfwi_barrier_selftest: the persistent kernels' grid barrier
+        waiting for a CTA that does not exist gives up after limit_ns and sets
+        the error word to 3 (read by check_device)."""
+        N.check(self.lib.pyfwi_barrier_selftest(self.handle, self.ws, self.ws_bytes, int(limit_ns),
+                                                _stream(self.device)))
 
     def profile(self, enable=True):
         """Bracket every step kernel with CUDA events (see profile_read)."""

@@ -130,17 +130,44 @@ def lowpass_response(nt, highcut, fn, order=1):
     return np.ascontiguousarray(g[idx], np.float32)
 
 
-def _device_response(nt, highcut, fn, order, device):
+def lowpass_spectrum(nt, highcut, fn, order=1):
+    """The operator of lowpass_response applied by FFT: (nfft, filter) with
+    nfft the smallest power of two >= 2 nt - 1 and filter the float32 array
+    pyfwi_lowpass takes: the real spectrum of the response embedded in a
+    circulant of nfft points (c[k] = c[nfft - k] = g[k] for k < nt, zero
+    between), divided by nfft, followed by the twiddles exp(-2 pi i j / nfft),
+    j < nfft / 2, as (cos, sin) pairs.  The product of a zero-padded trace's
+    FFT with that spectrum, transformed back, is K x on the first nt
+    samples."""
+    from scipy.signal import butter, freqz
+    nt = int(nt)
+    n = nt + LOWPASS_PADDING
+    b, a = butter(order, 2 * highcut / fn, btype="lowpass", output="ba")
+    _, h = freqz(b, a, worN=n, whole=True)
+    g = np.fft.ifft(np.conjugate(h) * h).real
+    nfft = 1 << max(1, int(np.ceil(np.log2(2 * nt - 1))) if nt > 1 else 1)
+    c = np.zeros(nfft)
+    c[:nt] = g[:nt]
+    c[nfft - nt + 1:] = g[1:nt][::-1]
+    spec = np.fft.fft(c).real / nfft
+    j = np.arange(nfft // 2)
+    tw = np.stack([np.cos(2 * np.pi * j / nfft), -np.sin(2 * np.pi * j / nfft)], 1).reshape(-1)
+    return nfft, np.ascontiguousarray(np.concatenate([spec, tw]), np.float32)
+
+
+def _device_filter(nt, highcut, fn, order, device):
     import torch
     key = (int(nt), float(highcut), float(fn), int(order), str(device))
     if key not in _RESPONSES:
-        _RESPONSES[key] = torch.from_numpy(lowpass_response(nt, highcut, fn, order)).to(device)
+        nfft, f = lowpass_spectrum(nt, highcut, fn, order)
+        _RESPONSES[key] = (nfft, torch.from_numpy(f).to(device))
     return _RESPONSES[key]
 
 
 def _filter(x, highcut, fn, order, axis):
     """Filter (n_planes, nt, ncols) traces along axis 1 on the device
-    (pyfwi_lowpass); numpy in, numpy out (float64, as the reference)."""
+    (pyfwi_lowpass: FFT convolution with the response, one kernel launch);
+    numpy in, numpy out (float64, as the reference)."""
     import torch
     from . import _native as N
     from .engine import _ptr, _stream
@@ -155,9 +182,9 @@ def _filter(x, highcut, fn, order, axis):
         t = t[None]
     t = t.reshape(t.shape[0], t.shape[1], -1)  # (planes, nt, traces): '3d' sections too
     out = torch.empty_like(t)
-    K = _device_response(t.shape[1], highcut, fn, order, dev)
-    N.check(N.lib().pyfwi_lowpass(_ptr(K), _ptr(t), _ptr(out), int(t.shape[1]), int(t.shape[2]), int(t.shape[0]),
-                                  _stream(dev)))
+    nfft, filt = _device_filter(t.shape[1], highcut, fn, order, dev)
+    N.check(N.lib().pyfwi_lowpass(_ptr(filt), nfft, _ptr(t), _ptr(out), int(t.shape[1]), int(t.shape[2]),
+                                  int(t.shape[0]), _stream(dev)))
     out = out.reshape(shape)
     return out.cpu().numpy().astype(np.float64) if as_numpy else out
 

@@ -13,16 +13,23 @@ torch tensors (outputs stay on the device).
 Extra ``inpa`` keys (all optional): ``checkpoint`` ('exact' or 'reverse';
 default: 'exact' when chpr == 100, else the reference's reverse-time scheme),
 ``segment`` (steps per recompute segment), ``shot_batch``, ``tile`` (step
-kernel variant, 0..5, or 'auto' to time them all on this survey first and
+kernel variant, 0..7 -- tile kernels of 16 / 8 / 32 rows, streaming kernels
+of 128 / 64 / 256 columns, 16-row tile kernels whose adjoint CTAs carry 2 / 4
+shots -- or 'auto' to time them all on this survey first and
 take the fastest forward and adjoint variant), ``adj_tile`` (adjoint step
 variant when it differs from ``tile``), ``chunk`` (rows per CTA of the
 streaming variants), ``graph`` (replay whole calls as CUDA graphs: True,
 False, or 'auto', the default: on where a launch carries at most 8 M
 cell-shots, where issuing launches from the host would cost a noticeable
-share),
-``snapshot`` ('fp32', or 'bf16': the forward states the imaging reads are
-stored in BF16 while the forward recurrence stays FP32; halves their memory
-and their reads at the cost of rounding the imaged fields to 8 bits),
+share), ``persist`` (run the time loops as persistent cooperative kernels,
+many steps per launch with a grid barrier between steps, where the layout
+stores every step in FP32 and the tile kernels run: True, False, or 'auto',
+the default: on where a step carries at most 2 M cell-shots),
+``snapshot`` ('fp32'; 'bf16': the forward states the imaging reads are
+stored in BF16 while the forward recurrence stays FP32, halving their memory
+and their reads at the cost of rounding the imaged fields to 8 mantissa bits;
+'fp24': the same with a byte plane widening BF16 to 15 mantissa bits, three
+quarters of the FP32 store),
 ``adjoint`` ('reference': PyFWI's gradient, masked and normalised as
 gradient_reading does; 'exact': the exact derivative of
 J = 1/2 sum (section - observed)^2 of this library's discrete forward step on
@@ -133,6 +140,10 @@ class WavePreparation:
         # cap in bytes on the device memory the layout may plan for (None:
         # what is free when the plan is built); SurveyBatch shares memory out
         self.memory_budget = None
+        # False keeps the time loops one launch per step whatever
+        # inpa['persist'] says (SurveyBatch runs surveys side by side, where
+        # cooperative grids would compete for the SMs)
+        self.persist_allowed = True
 
     @property
     def plan(self):
@@ -280,6 +291,7 @@ class WavePreparation:
             o.tile, o.adj_tile = variants
             o.adjoint = N.ADJOINT_EXACT if self.adjoint == "exact" else N.ADJOINT_REFERENCE
             o.graph = int(self._graph_on(inpa.get("graph", "auto"), batch))
+            o.persist = int(self._persist_on(inpa.get("persist", "auto"), batch))
             o.chunk = int(inpa.get("chunk", 0))
             if chp is not None:
                 o.nchp = int(chp.size)
@@ -292,9 +304,10 @@ class WavePreparation:
         if self.adjoint == "exact" and mode != "exact":
             raise ValueError("inpa['adjoint'] = 'exact' needs checkpoint 'exact'")
         snap = inpa.get("snapshot", "fp32")
-        if snap not in ("fp32", "bf16") or (snap == "bf16" and mode != "exact"):
-            raise ValueError("inpa['snapshot'] must be 'fp32' or 'bf16' (bf16 with checkpoint 'exact' only)")
-        snapshot = N.SNAP_BF16 if snap == "bf16" else N.SNAP_FP32
+        if snap not in ("fp32", "bf16", "fp24") or (snap != "fp32" and mode != "exact"):
+            raise ValueError("inpa['snapshot'] must be 'fp32', 'bf16' or 'fp24' (the last two with checkpoint "
+                             "'exact' only)")
+        snapshot = {"fp32": N.SNAP_FP32, "bf16": N.SNAP_BF16, "fp24": N.SNAP_FP24}[snap]
         self.snapshot = snap
         tile = inpa.get("tile", DEFAULT_TILE)
         adj_tile = inpa.get("adj_tile", None)
@@ -318,6 +331,22 @@ class WavePreparation:
     # 1.08x); above it the kernels hide the issue cost and the copies into
     # the captured buffers are pure overhead
     GRAPH_AUTO_CELLS = 8_000_000
+
+    # 'auto' runs the time loops as persistent kernels (many steps per
+    # cooperative launch, a grid barrier between steps) where a step carries
+    # at most this many cell-shots: there each step kernel runs for
+    # microseconds and the launches, not the steps, set the pace
+    PERSIST_AUTO_CELLS = 2_000_000
+
+    def _persist_on(self, persist, batch):
+        if not self.persist_allowed:
+            return False
+        if persist == "auto":
+            b = int(batch) if batch else int(self.ns)
+            return int(self.tnz) * int(self.tnx) * b <= self.PERSIST_AUTO_CELLS
+        if persist not in (True, False, 0, 1):
+            raise ValueError("inpa['persist'] must be True, False or 'auto'")
+        return bool(persist)
 
     def _graph_on(self, graph, batch):
         if graph == "auto":
@@ -439,13 +468,14 @@ class WavePropagator(WavePreparation):
         return self._damp_dev
 
     def _check_device(self, synchronous):
-        """Raise if a streaming kernel stopped early.  Reading the error word
-        synchronises, so it is done where the call synchronises anyway (host
-        results) or where a streaming kernel ran, never inside a CUDA-graph
-        capture."""
+        """Raise if a streaming or persistent kernel stopped early.  Reading
+        the error word synchronises, so it is done where the call synchronises
+        anyway (host results) or where such a kernel may have run, never
+        inside a CUDA-graph capture."""
         if torch.cuda.is_current_stream_capturing():
             return
-        if synchronous or self.plan.opts.tile >= 3 or self.plan.opts.adj_tile >= 4:
+        o = self.plan.opts
+        if synchronous or 3 <= o.tile <= 5 or 4 <= o.adj_tile <= 6 or o.persist:
             self.plan.check_device()
 
     def _section(self, traces):

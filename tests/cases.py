@@ -375,3 +375,62 @@ def timelapse(method):
 
 
 TL_METHODS = ["pa", "cc", "dd", "sim", "wa", "cj", "cd", "cu"]
+
+
+def _cut_record(case, nt):
+    """The case with its record cut to nt trace samples (same dt)."""
+    case = dict(case)
+    case["inpa"] = dict(case["inpa"], t=_t_for(nt, case["inpa"]["dt"]))
+    return case
+
+
+def c2_parity():
+    """The 200 x 400 survey exactly as configured (10 shots, nt = 2000):
+    its fixture holds the reference's gradient on the whole survey."""
+    case = c2()
+    case["name"] = "c2_parity"
+    return case
+
+
+def c3_parity(nt=1200, shots=(20, 45)):
+    """The 560 x 1060 padded grid of the 64-shot survey, two of its shots
+    (x = 320 and 695 cells), the record cut to nt samples.  The product runs
+    it with the 64-shot layout of the full survey: the two shots repeated 32
+    times, all 64 in one launch, 157-step recompute segments."""
+    case = c3(ns=64)
+    case = _cut_record(case, nt)
+    case["src_loc"] = case["src_loc"][list(shots)].copy()
+    case["name"] = "c3_parity"
+    return case
+
+
+def c4_parity(n_samples=400, n_shots=2):
+    """The largest sub-stepped model of the uneven batch (c4_08: 397 x 987
+    cells, dh 9.26 m, dt 1.30 ms split into three internal steps), its first
+    and last shots, the record cut to n_samples samples."""
+    case = c4()[8]
+    case = _cut_record(case, n_samples)
+    idx = [0, len(case["src_loc"]) - 1][:n_shots]
+    case["src_loc"] = case["src_loc"][idx].copy()
+    case["name"] = "c4_parity"
+    return case
+
+
+def c5_parity(nz=300, nx=800, nt=1200):
+    """The thrust-belt survey cropped to its top-left nz x nx cells (40-cell
+    water layer with vs = 0 included, same 40-cell absorbing layer, dh, dt,
+    6 Hz wavelet and receiver spacing), two shots, the record cut to nt
+    samples."""
+    case = c5(ns=128)
+    case = _cut_record(case, nt)
+    for key in ("model_obs", "model_est", "model_mon"):
+        case[key] = {k: np.ascontiguousarray(v[:nz, :nx]) for k, v in case[key].items()}
+    rec = case["rec_loc"]
+    case["rec_loc"] = rec[rec[:, 0] < (nx - 1) * case["inpa"]["dh"]].copy()
+    dh = case["inpa"]["dh"]
+    case["src_loc"] = np.array([[200 * dh, 2 * dh], [560 * dh, 2 * dh]], np.float32)
+    case["name"] = "c5_parity"
+    return case
+
+
+LARGE = [c2_parity, c3_parity, c4_parity, c5_parity]  # reference fixtures at the configured sizes

@@ -55,3 +55,19 @@ def fp64_propagator(case, precision="fp64"):
     return O.OracleWavePropagator(inpa, src, case["rec_loc"], case["model_est"]["vp"].shape,
                                   components=case["components"], n_well_rec=case["n_well_rec"], chpr=100,
                                   precision=precision)
+
+
+def input_digest(case):
+    """sha256 over the models, geometry and wavelet parameters of a case: a
+    fixture stores it so a test can tell that tests/cases.py still builds
+    the survey the fixture was made from."""
+    import hashlib
+    h = hashlib.sha256()
+    for key in ("model_obs", "model_est"):
+        for k in ("vp", "vs", "rho"):
+            h.update(np.ascontiguousarray(case[key][k], np.float32).tobytes())
+    h.update(np.ascontiguousarray(case["src_loc"], np.float32).tobytes())
+    h.update(np.ascontiguousarray(case["rec_loc"], np.float32).tobytes())
+    h.update(repr(sorted(case["inpa"].items())).encode())
+    h.update(repr((case["fdom"], case["src_type"], case["components"], case["chpr"])).encode())
+    return h.hexdigest()

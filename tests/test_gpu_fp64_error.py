@@ -21,6 +21,7 @@ pytestmark = pytest.mark.gpu
 
 NAMES = ["c1"] + [f.__name__ for f in cases.TINY]
 BF16_GRAD_TOL = 1e-2
+FP24_GRAD_TOL = 1e-4  # the gradient bar of the configurations, against FP64
 
 
 def _fp64(name):
@@ -66,6 +67,37 @@ def test_bf16_snapshot_error_against_fp64(name):
     e32, e16 = _err(g32, f64, "grad_"), _err(g16, f64, "grad_")
     print("\n%s gradient vs FP64: fp32 snapshots %.2e, bf16 snapshots %.2e" % (name, e32, e16))
     assert e16 <= BF16_GRAD_TOL, e16
+
+
+@pytest.mark.parametrize("name", [n for n in NAMES if cases.by_name(n)["chpr"] == 100])
+def test_fp24_snapshot_error_against_fp64(name):
+    """24-bit snapshots (BF16 plus a byte: 15 mantissa bits) keep the
+    gradient within 1e-4 of the FP64 oracle on three quarters of the FP32
+    store; seismograms are bit-identical to FP32 snapshots."""
+    case = cases.by_name(name)
+    f64 = _fp64(name)
+    d32, g32 = _run(case, checkpoint="exact")
+    d24, g24 = _run(case, checkpoint="exact", snapshot="fp24")
+    for k in d32:
+        assert np.array_equal(d24[k], d32[k]), k
+    e32, e24 = _err(g32, f64, "grad_"), _err(g24, f64, "grad_")
+    print("\n%s gradient vs FP64: fp32 snapshots %.2e, fp24 snapshots %.2e" % (name, e32, e24))
+    assert e24 <= FP24_GRAD_TOL, e24
+
+
+def test_fp24_snapshots_on_the_200x400_survey():
+    """The torch-check configuration (10 shots, nt 2000): the gradient with
+    24-bit snapshots against the FP32-snapshot gradient and against the
+    reference's own gradient, both within 1e-4 (the FP32-snapshot gradient
+    is ~1e-5 from FP64 on every smaller case)."""
+    case = cases.c2_parity()
+    ref = load_golden("c2_parity")
+    _, g32 = _run(case, checkpoint="exact")
+    _, g24 = _run(case, checkpoint="exact", snapshot="fp24")
+    e_32 = max(rel_l2(g24[k], g32[k]) for k in g24)
+    e_ref = max(rel_l2(g24[k], ref["grad_" + k]) for k in g24)
+    print("\nc2 fp24 snapshots: %.2e from fp32 snapshots, %.2e from the reference" % (e_32, e_ref))
+    assert e_32 <= FP24_GRAD_TOL and e_ref <= FP24_GRAD_TOL, (e_32, e_ref)
 
 
 def test_bf16_snapshots_with_segments_and_batches():

@@ -1,5 +1,6 @@
-"""The multiscale low-pass on the device (pyfwi_lowpass: the filter's nt x nt
-response as an FP32 GEMM) against the reference's outputs, and the
+"""The multiscale low-pass on the device (pyfwi_lowpass: FFT convolution of
+every trace with the filter's response, one kernel) against the reference's
+outputs, and the
 band-limited FWI misfit and gradient (FWI.fprime with a frequency) against
 the oracle's restatement of the reference pipeline: forward modelling,
 lowpass of both data, L2 residual, adj_lowpass, gradient."""
@@ -64,3 +65,22 @@ def test_band_limited_fprime_matches_oracle(name, freq):
     rms_o, grad_o = _oracle_fprime(case, d_obs, freq)
     assert abs(rms - rms_o) <= 1e-4 * abs(rms_o), (rms, rms_o)
     assert rel_l2(grad, grad_o) <= 1e-4, rel_l2(grad, grad_o)
+
+
+@pytest.mark.parametrize("planes,nt,ncols,hc", [(2, 6000, 7, 6.0), (3, 1537, 33, 25.0), (1, 150, 64, 60.0),
+                                                (2, 1, 5, 60.0), (1, 4000, 2001, 8.0)])
+def test_device_lowpass_shapes_match_oracle(planes, nt, ncols, hc):
+    """The FFT kernel on record lengths from 1 to 6000 samples (FFTs of 2 to
+    16384 points, 1 to 4 trace pairs per CTA), odd trace counts (a CTA with
+    an unpaired trace) and several planes, against the oracle's
+    restatement of the reference's filter."""
+    import torch
+    import oracle as O
+    from pyfwi_b200 import fwi_tools
+    rng = np.random.default_rng(nt + ncols)
+    x = rng.standard_normal((planes, nt, ncols)).astype(np.float32)
+    y = fwi_tools.lowpass(torch.from_numpy(x).cuda(), hc, FN, order=3, axis=1)
+    ref = O.lowpass(x, hc, FN, 3)
+    assert rel_l2(y.cpu().numpy(), ref) < 1e-5, rel_l2(y.cpu().numpy(), ref)
+    for p in range(planes):  # each plane on its own too
+        assert rel_l2(y[p].cpu().numpy(), ref[p]) < 1e-5

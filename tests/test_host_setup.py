@@ -103,3 +103,27 @@ def test_gaussian_weights_follow_scipy():
         x = np.zeros(4 * r + 9)
         x[2 * r + 4] = 1.0
         np.testing.assert_allclose(gaussian_filter1d(x, sigma), np.convolve(x, w, mode="same"), rtol=0, atol=1e-15)
+
+
+LARGE = [f.__name__ for f in cases.LARGE]
+
+
+@pytest.mark.parametrize("name", LARGE)
+def test_setup_matches_reference_at_configured_sizes(name):
+    """The same set-up values on the surveys of the configured sizes (the
+    sub-stepped one included), and the fixture was made from the inputs
+    tests/cases.py builds."""
+    from helpers import input_digest
+    g = load_golden(name)
+    case = cases.by_name(name)
+    assert input_digest(case) == str(g["in_sha"])
+    W = product(case)
+    assert np.array_equal(W.chp, g["setup_chp"])
+    assert W.nt == int(g["setup_nt"]) and W.nt_ext == int(g["setup_nt_ext"])
+    assert float(W.dt_scale) == float(g["setup_dt_scale"]) and W.dt == float(g["setup_dt"])
+    assert np.array_equal(W.srcx, g["setup_srcx"]) and np.array_equal(W.srcz, g["setup_srcz"])
+    assert int(W.dxr) == int(g["setup_dxr"]) and int(W.sdo) == int(g["setup_sdo"])
+    for k in ("rec_top_left_const", "rec_top_left_var", "rec_top_right_const", "rec_top_right_var",
+              "rec_surface_const", "rec_surface_var", "src_cts"):
+        assert int(getattr(W, k)) == int(g["setup_" + k]), k
+    assert np.array_equal(W.src.w, g["setup_wavelet"])

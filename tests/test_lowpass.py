@@ -1,7 +1,10 @@
 """The multiscale low-pass (lowpass / adj_lowpass, fwi_tools.py:1188-1258)
 on the CPU: the oracle's restatement reproduces the reference's outputs
-(tests/golden/lowpass.npz, make_lowpass.py), and the nt x nt response the
-device applies (pyfwi_b200.fwi_tools.lowpass_response) is the same operator."""
+(tests/golden/lowpass.npz, make_lowpass.py); the nt x nt response
+(pyfwi_b200.fwi_tools.lowpass_response) is the same operator, and so is
+the spectrum the device's FFT kernel applies (lowpass_spectrum), here
+applied with numpy's FFT exactly as the kernel does: two traces per complex
+signal, zero-padded to nfft, times the real spectrum, transformed back."""
 import os
 
 import numpy as np
@@ -37,3 +40,26 @@ def test_response_matrix_is_the_reference_filter():
         y = np.einsum("ts,psc->ptc", K, x)
         ref = f["low%d" % q]
         assert np.linalg.norm(y - ref) <= 1e-6 * np.linalg.norm(ref)
+
+
+def test_spectrum_is_the_reference_filter():
+    from pyfwi_b200.fwi_tools import lowpass_spectrum
+    f = _fixture()
+    for q in range(2):
+        x, hc = f["x%d" % q].astype(np.float64), float(f["hc%d" % q])
+        planes, nt, ncols = x.shape
+        nfft, filt = lowpass_spectrum(nt, hc, FN, 3)
+        assert nfft >= 2 * nt - 1 and nfft & (nfft - 1) == 0 and filt.shape == (2 * nfft,)
+        spec = filt[:nfft].astype(np.float64)
+        tw = filt[nfft:].reshape(-1, 2)
+        j = np.arange(nfft // 2)
+        assert np.allclose(tw[:, 0], np.cos(2 * np.pi * j / nfft), atol=1e-7)
+        assert np.allclose(tw[:, 1], -np.sin(2 * np.pi * j / nfft), atol=1e-7)
+        xp = np.zeros((planes, nfft, ncols + ncols % 2))
+        xp[:, :nt, :ncols] = x
+        z = xp[..., 0::2] + 1j * xp[..., 1::2]  # traces 2p and 2p + 1 in one complex signal
+        w = np.fft.ifft(np.fft.fft(z, axis=1) * spec[None, :, None], axis=1) * nfft
+        y = np.empty_like(xp[:, :nt])
+        y[..., 0::2], y[..., 1::2] = w.real[:, :nt], w.imag[:, :nt]
+        ref = f["low%d" % q]
+        assert np.linalg.norm(y[..., :ncols] - ref) <= 1e-6 * np.linalg.norm(ref)

@@ -36,59 +36,94 @@ def _bind():
     return N, L
 
 
-def test_static_scratch_gradient_matches_workspace_path():
-    import torch
-    from pyfwi_b200.engine import Plan
+class _Survey:
+    """One case set up twice: the regular path (caller-owned workspace:
+    pyfwi_set_model, pyfwi_forward, pyfwi_l2_residual per observed
+    component, pyfwi_gradient) and a plan for the static-scratch entry
+    point; `observed` lists the raw components in the misfit (the others
+    are passed as NULL)."""
 
-    N, L = _bind()
-    case = cases.tiny_s8()
-    g = load_golden("tiny_s8")
-    W = product(case, segment=0, shot_batch=0)
-    geom = W._geometry()
-    dev = torch.device("cuda", 0)
-    stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    def __init__(self, name, observed, energy):
+        import torch
+        from pyfwi_b200.engine import Plan
+        N, L = _bind()
+        self.N, self.L = N, L
+        case = cases.by_name(name)
+        g = load_golden(name)
+        W = product(case, segment=0, shot_batch=0)
+        geom = W._geometry()
+        dev = torch.device("cuda", 0)
+        self.stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
 
-    def opts():
-        o = N.Options()
-        o.checkpoint, o.snapshot, o.energy, o.tile = N.CKPT_EXACT, N.SNAP_FP32, 1, 0
-        return o
+        def opts():
+            o = N.Options()
+            o.checkpoint, o.snapshot, o.energy, o.tile = N.CKPT_EXACT, N.SNAP_FP32, energy, 0
+            return o
 
-    model = [torch.from_numpy(np.ascontiguousarray(case["model_est"][k])).to(dev) for k in ("vp", "vs", "rho")]
-    damp = [torch.from_numpy(np.ascontiguousarray(W.dx_pml[0, :])).to(dev),
-            torch.from_numpy(np.ascontiguousarray(W.dz_pml[:, 0])).to(dev)]
-    obs = [torch.from_numpy(np.ascontiguousarray(g["d_obs_" + k])).to(dev) for k in FIELDS]
-    src = np.ascontiguousarray(W._wavelet, np.float32)
+        self.model = [torch.from_numpy(np.ascontiguousarray(case["model_est"][k])).to(dev)
+                      for k in ("vp", "vs", "rho")]
+        self.damp = [torch.from_numpy(np.ascontiguousarray(W.dx_pml[0, :])).to(dev),
+                     torch.from_numpy(np.ascontiguousarray(W.dz_pml[:, 0])).to(dev)]
+        self.obs = [torch.from_numpy(np.ascontiguousarray(g["d_obs_" + k])).to(dev) if k in observed else None
+                    for k in FIELDS]
+        self.src = np.ascontiguousarray(W._wavelet, np.float32)
+        self.shape = (3, int(W.nz), int(W.nx))
+        self.dev = dev
 
-    # regular path: caller-owned workspace
-    A = Plan(geom, W.srcx, W.srcz, opts(), dev)
-    A.set_model(*model, *damp)
-    traces = A.forward(src)
-    misfit_a = torch.zeros((), dtype=torch.float64, device=dev)
-    scratch = torch.empty(N.REDUCE_SLOTS, dtype=torch.float64, device=dev)
-    res = []
-    for c in range(5):
-        r = torch.empty_like(obs[c])
-        N.check(L.pyfwi_l2_residual(_p(traces[c]), _p(obs[c]), _p(r), r.numel(), _p(scratch), _p(misfit_a),
-                                    stream))
-        res.append(r)
-    grad_a = A.gradient(res, N.PARAM_LMD)
-    torch.cuda.synchronize()
+        # regular path
+        A = Plan(geom, W.srcx, W.srcz, opts(), dev)
+        A.set_model(*self.model, *self.damp)
+        traces = A.forward(self.src)
+        self.misfit = torch.zeros((), dtype=torch.float64, device=dev)
+        scratch = torch.empty(N.REDUCE_SLOTS, dtype=torch.float64, device=dev)
+        res = []
+        for c in range(5):
+            if self.obs[c] is None:
+                res.append(None)
+                continue
+            r = torch.empty_like(self.obs[c])
+            N.check(L.pyfwi_l2_residual(_p(traces[c]), _p(self.obs[c]), _p(r), r.numel(), _p(scratch),
+                                        _p(self.misfit), self.stream))
+            res.append(r)
+        self.grad = A.gradient(res, N.PARAM_LMD)
+        torch.cuda.synchronize()
+        self.B = Plan(geom, W.srcx, W.srcz, opts(), dev)
 
-    # the static-scratch entry point, twice on the same plan
-    B = Plan(geom, W.srcx, W.srcz, opts(), dev)
-    observed = (ctypes.c_void_p * 5)(*[o.data_ptr() for o in obs])
-    for call in range(2):
-        grad_b = torch.full((3, int(W.nz), int(W.nx)), float("nan"), dtype=torch.float32, device=dev)
-        misfit_b = torch.full((), float("nan"), dtype=torch.float64, device=dev)
-        rc = L.pyfwi_gradient_static(B.handle, *[_p(t) for t in model], *[_p(t) for t in damp],
-                                     src.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(src.shape[0]),
-                                     observed, N.PARAM_LMD, _p(grad_b), _p(misfit_b), stream)
-        assert rc == 0, L.pyfwi_last_error()
+    def static_call(self):
+        """One pyfwi_gradient_static call; checks it against the regular path."""
+        import torch
+        observed = (ctypes.c_void_p * 5)(*[o.data_ptr() if o is not None else None for o in self.obs])
+        grad = torch.full(self.shape, float("nan"), dtype=torch.float32, device=self.dev)
+        misfit = torch.full((), float("nan"), dtype=torch.float64, device=self.dev)
+        rc = self.L.pyfwi_gradient_static(self.B.handle, *[_p(t) for t in self.model], *[_p(t) for t in self.damp],
+                                          self.src.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                          int(self.src.shape[0]), observed, self.N.PARAM_LMD, _p(grad), _p(misfit),
+                                          self.stream)
+        assert rc == 0, self.L.pyfwi_last_error()
         torch.cuda.synchronize()
         for q in range(3):
-            assert rel_l2(grad_b[q].cpu().numpy(), grad_a[q].cpu().numpy()) <= GRAD_TOL, (call, q)
+            assert rel_l2(grad[q].cpu().numpy(), self.grad[q].cpu().numpy()) <= GRAD_TOL, q
         # the same reductions in the same order: the same bits
-        assert float(misfit_b) == float(misfit_a), call
+        assert float(misfit) == float(self.misfit)
+
+
+def test_static_scratch_gradient_matches_workspace_path():
+    """Two calls in a row on one plan, every component observed."""
+    s = _Survey("tiny_s8", FIELDS, energy=1)
+    s.static_call()
+    s.static_call()
+
+
+def test_static_scratch_shared_between_plans():
+    """The array is shared: a plan of another geometry (and shot count)
+    uses it between two calls of the first, and some components are left
+    out of the misfit (NULL observed pointers, so fewer residual planes)."""
+    a = _Survey("tiny_s8", ["vx", "tauz"], energy=1)
+    b = _Survey("tiny_dxr", ["vx", "vz"], energy=0)
+    a.static_call()
+    b.static_call()
+    a.static_call()
+    b.static_call()
 
 
 def test_static_scratch_rejects_oversized_surveys():
