@@ -545,7 +545,9 @@ struct StepVar {
 // floats of shared memory.  Ends with shared memory still in use: a caller
 // that reuses it for another tile synchronises first.
 // W24: snapshots are written as 24 bits (sv.snap8 set), else as BF16.
-template <int R, int TZ, bool W24, class V>
+// STAGED: the caller has put the tile's input in shared memory already (the
+// TMA kernel); otherwise it is copied here with cp.async.
+template <int R, int TZ, bool W24, class V, bool STAGED = false>
 __device__ __forceinline__ void fwd_tile(const StepArgs &a, const V &sv, int bx, int by, int slot, float *sm)
 {
     using S = FwdShape<R, TZ>;
@@ -564,27 +566,29 @@ __device__ __forceinline__ void fwd_tile(const StepArgs &a, const V &sv, int bx,
     const float dt = a.k.dt;
 
     // every copy of the tile in flight at once, then one wait
-    for (int e = tid; e < HT * (SW / 4); e += NTHREADS) {
+    for (int e = tid; !STAGED && e < HT * (SW / 4); e += NTHREADS) {
         int r = e / (SW / 4), q = e - r * (SW / 4);
         int gi = i0 - 2 * R + r, gj = j0 - 8 + 4 * q, o = r * SW + 4 * q;
         cp4(s_txx + o, in + TXX * P, g, gi, gj);
         cp4(s_tzz + o, in + TZZ * P, g, gi, gj);
         cp4(s_txz + o, in + TXZ * P, g, gi, gj);
     }
-    for (int e = tid; e < HV * (VW / 4); e += NTHREADS) {
+    for (int e = tid; !STAGED && e < HV * (VW / 4); e += NTHREADS) {
         int r = e / (VW / 4), q = e - r * (VW / 4);
         int gi = i0 - R + r, gj = j0 - 4 + 4 * q, o = r * VW + 4 * q;
         cp4(s_vx + o, in + VX * P, g, gi, gj);
         cp4(s_vz + o, in + VZ * P, g, gi, gj);
         cp4(s_b + o, a.mat + 2 * P, g, gi, gj);
     }
-    for (int e = tid; e < TZ * (TX / 4); e += NTHREADS) {
+    for (int e = tid; !STAGED && e < TZ * (TX / 4); e += NTHREADS) {
         int r = e / (TX / 4), q = e - r * (TX / 4), o = r * TX + 4 * q;
         cp4(s_lam + o, a.mat, g, i0 + r, j0 + 4 * q);
         cp4(s_mu + o, a.mat + P, g, i0 + r, j0 + 4 * q);
     }
-    cp_wait_all();
-    __syncthreads();
+    if (!STAGED) {
+        cp_wait_all();
+        __syncthreads();
+    }
     if (sv.add_src && tid == 0) {  // wave_propagation.py:652-664, elastic_surface.cl:23-28
         const int si = a.srcz[shot], sj = a.srcx[shot];
         const int ct = sj - (j0 - 8), cv = sj - (j0 - 4), rt = si - (i0 - 2 * R), rv = si - (i0 - R);

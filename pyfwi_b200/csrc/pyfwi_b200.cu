@@ -9,6 +9,7 @@
 #include "kernels.cuh"
 #include "persist_kernels.cuh"
 #include "stream_kernels.cuh"
+#include "tile_tma.cuh"
 
 #include <nvtx3/nvToolsExt.h>
 
@@ -64,11 +65,14 @@ size_t up(size_t x, size_t a = ALIGN) { return (x + a - 1) / a * a; }
 // kernel variants: 0..2 tile kernels with 16 / 8 / 32 rows per tile,
 // 3..5 streaming kernels whose CTAs span 128 / 64 / 256 columns, 6..7 the
 // 16-row tile kernels whose adjoint CTAs carry 2 / 4 shots each (the
-// forward step of 6..7 is variant 0's)
-constexpr int TILE_TZ[] = {16, 8, 32, 0, 0, 0, 16, 16};
-constexpr int STREAM_W[] = {0, 0, 0, 128, 64, 256, 0, 0};
-constexpr int ADJ_NS[] = {1, 1, 1, 1, 1, 1, 2, 4};
-constexpr int N_TILES = 8;
+// forward step of 6..7 is variant 0's), 8..10 the tile kernels of 16 / 8 /
+// 32 rows with the forward tile staged by TMA box copies (the adjoint of
+// 8..10 is that of 0..2)
+constexpr int TILE_TZ[] = {16, 8, 32, 0, 0, 0, 16, 16, 16, 8, 32};
+constexpr int STREAM_W[] = {0, 0, 0, 128, 64, 256, 0, 0, 0, 0, 0};
+constexpr int ADJ_NS[] = {1, 1, 1, 1, 1, 1, 2, 4, 1, 1, 1};
+constexpr int FWD_TMA[] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1};
+constexpr int N_TILES = 11;
 constexpr int FWD_PF = 4, ADJ_PF = 2;  // rows the streaming kernels fetch ahead
 constexpr size_t ERR_OFF = 128;         // byte offset of the device error word in the header
 constexpr size_t CHECK_OFF = 192;       // byte offset of the frame-check counter (uint64) in the header
@@ -94,7 +98,7 @@ struct pyfwi_plan {
     Grid g;
     Coef k;
     Lines lines;
-    int R, tz, st_w, atz, ast_w, ans, chunk_opt, nacc, G, ngroups, seg, M, n_inj;  // a*: adjoint step variant
+    int R, tz, st_w, ftma, atz, ast_w, ans, chunk_opt, nacc, G, ngroups, seg, M, n_inj;  // a*: adjoint step variant
     bool exact_adj = false;  // PYFWI_ADJOINT_EXACT
     bool persist = false;    // time loops as persistent kernels (options.persist, where the layout allows)
     int fwd_cap = 0, adj_cap = 0;  // co-resident CTAs of the persistent kernels on this device
@@ -122,12 +126,13 @@ struct pyfwi_plan {
         long long launches = 0;
     } gfwd, ggrad, gmis;
     cudaStream_t cap = nullptr;  // capture stream (the caller's may be the legacy default stream)
-    // tensor map of the workspace for the streaming kernels, per box width
+    // tensor maps of the workspace (rows of `pitch` floats), per box shape
     struct TMap {
         void *ws = nullptr;
-        int w = 0;
+        int w = 0, h = 0;
         alignas(64) CUtensorMap map;
-    } tmaps[2];
+    } tmaps[6];
+    int tmap_next = 0;
 };
 
 // The static-scratch entry point clears its array before every call: the
@@ -343,17 +348,17 @@ int stream_chunk(const pyfwi_plan *p, int nslots, int T)
 }
 
 // The workspace as a 2-D tensor of rows of `pitch` floats with a box of
-// W x 1, for the streaming kernels; encoded once per workspace and width.
-int workspace_map(pyfwi_plan *p, const float *ws, int W, CUtensorMap *out)
+// W x H (W x 1 for the streaming kernels, whole tiles for the TMA tile
+// kernel); encoded once per workspace and box, a few kept.
+int workspace_map(pyfwi_plan *p, const float *ws, int W, CUtensorMap *out, int H = 1)
 {
-    pyfwi_plan::TMap *slot = nullptr;
     for (auto &m : p->tmaps)
-        if (m.ws == ws && m.w == W) {
+        if (m.ws == ws && m.w == W && m.h == H) {
             *out = m.map;
             return PYFWI_OK;
         }
-    slot = &p->tmaps[p->tmaps[0].ws ? 1 : 0];
-    if (p->tmaps[0].ws && p->tmaps[1].ws) slot = &p->tmaps[0];
+    pyfwi_plan::TMap *slot = &p->tmaps[p->tmap_next];
+    p->tmap_next = (p->tmap_next + 1) % (int)(sizeof p->tmaps / sizeof p->tmaps[0]);
     static EncodeTiled encode = nullptr;
     if (!encode) {
         void *fn = nullptr;
@@ -366,14 +371,45 @@ int workspace_map(pyfwi_plan *p, const float *ws, int W, CUtensorMap *out)
     const size_t row = (size_t)p->g.pitch * sizeof(float);
     cuuint64_t dims[2] = {(cuuint64_t)p->g.pitch, (cuuint64_t)(p->total / row)};
     cuuint64_t strides[1] = {(cuuint64_t)row};
-    cuuint32_t box[2] = {(cuuint32_t)W, 1}, estr[2] = {1, 1};
+    cuuint32_t box[2] = {(cuuint32_t)W, (cuuint32_t)H}, estr[2] = {1, 1};
     CUresult r = encode(&slot->map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(ws), dims, strides, box,
                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(PYFWI_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     slot->ws = const_cast<float *>(ws);
     slot->w = W;
+    slot->h = H;
     *out = slot->map;
+    return PYFWI_OK;
+}
+
+template <int R, int TZ>
+int launch_fwd_tma(pyfwi_plan *p, const StepArgs &a, int nslots, cudaStream_t s, const float *ws)
+{
+    using S = FwdShape<R, TZ>;
+    FwdTmaArgs t;
+    memset(&t, 0, sizeof t);
+    t.a = a;
+    t.a.tbase = ws;
+    t.a.err = at<int>(const_cast<float *>(ws), ERR_OFF);
+    int rc = workspace_map(p, ws, S::SW, &t.ms, S::HT);
+    if (!rc) rc = workspace_map(p, ws, S::VW, &t.mv, S::HV);
+    if (!rc) rc = workspace_map(p, ws, TX, &t.mt, TZ);
+    if (rc) return rc;
+    dim3 grid((p->g.tnx + TX - 1) / TX, (p->g.tnz + TZ - 1) / TZ, nslots);
+    const size_t sm = FwdTmaShape<R, TZ>::BYTES;
+    static bool attr = false;
+    if (!attr) {
+        CK(cudaFuncSetAttribute(fwd_tma<R, TZ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        CK(cudaFuncSetAttribute(fwd_tma<R, TZ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        attr = true;
+    }
+    if (a.snap8)
+        fwd_tma<R, TZ, true><<<grid, NTHREADS, sm, s>>>(t);
+    else
+        fwd_tma<R, TZ, false><<<grid, NTHREADS, sm, s>>>(t);
+    p->launches++;
+    CKL();
     return PYFWI_OK;
 }
 
@@ -441,6 +477,12 @@ int step_fwd(pyfwi_plan *p, const StepArgs &a, int nslots, cudaStream_t s, bool 
 #undef CASE
     }
     const int tz = p->tz ? p->tz : 16;  // reverse steps always use the tile kernel
+    if (p->ftma && !reverse) {
+#define CASE(R_, TZ_) \
+    if (p->R == R_ && tz == TZ_) return launch_fwd_tma<R_, TZ_>(p, a, nslots, s, ws);
+        CASE(2, 16) CASE(2, 8) CASE(2, 32) CASE(4, 16) CASE(4, 8) CASE(4, 32)
+#undef CASE
+    }
 #define CASE(R_, TZ_) \
     if (p->R == R_ && tz == TZ_) return launch_fwd<R_, TZ_>(p, a, nslots, s, reverse);
     CASE(2, 16) CASE(2, 8) CASE(2, 32) CASE(4, 16) CASE(4, 8) CASE(4, 32)
@@ -1211,6 +1253,7 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
     p->R = G.half_order;
     p->tz = TILE_TZ[opt->tile];
     p->st_w = STREAM_W[opt->tile];
+    p->ftma = FWD_TMA[opt->tile];
     const int av = opt->adj_tile ? opt->adj_tile - 1 : opt->tile;
     p->atz = TILE_TZ[av];
     p->ast_w = STREAM_W[av];
@@ -1255,7 +1298,8 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
     // persistent time loops: every step stored in FP32 (one segment), tile
     // kernels with one shot per adjoint CTA, the reference adjoint
     p->persist = opt->persist && opt->checkpoint == PYFWI_CKPT_EXACT && p->M == 1 &&
-                 opt->snapshot == PYFWI_SNAP_FP32 && !p->exact_adj && !p->st_w && !p->ast_w && p->ans == 1;
+                 opt->snapshot == PYFWI_SNAP_FP32 && !p->exact_adj && !p->st_w && !p->ftma && !p->ast_w &&
+                 p->ans == 1;
     if (p->persist) p->opt.graph = 0;  // a few launches per call: nothing to replay
 
     const size_t pf = (size_t)p->g.plane * sizeof(float), sb = (size_t)p->state * sizeof(float);

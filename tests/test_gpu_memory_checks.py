@@ -34,14 +34,16 @@ def _run(name, **extra):
     return W
 
 
-@pytest.mark.parametrize("tile", [0, 3])
+@pytest.mark.parametrize("tile", [0, 3, 7, 8])
 @pytest.mark.parametrize("name", NAMES)
 def test_no_write_outside_the_domains(name, tile):
     W = _run(name, tile=tile)
     assert W.plan.frame_check() == 0
 
 
-@pytest.mark.parametrize("extra", [{"tile": 1}, {"tile": 2}, {"tile": 4}, {"tile": 5}, {"tile": 0, "adj_tile": 3},
+@pytest.mark.parametrize("extra", [{"tile": 1}, {"tile": 2}, {"tile": 4}, {"tile": 5}, {"tile": 6}, {"tile": 9},
+                                   {"tile": 10}, {"persist": True, "segment": 0, "shot_batch": 0},
+                                   {"snapshot": "fp24", "segment": 7}, {"tile": 0, "adj_tile": 3},
                                    {"segment": 7, "shot_batch": 1}, {"snapshot": "bf16", "segment": 9},
                                    {"graph": True}, {"graph": False}])
 def test_no_write_outside_the_domains_variants(extra):
