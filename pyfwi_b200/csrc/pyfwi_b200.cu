@@ -656,6 +656,7 @@ int persist_backward(pyfwi_plan *p, void *ws, AdjArgs &a, int n, cudaStream_t st
     AdjPersistArgs pa;
     memset(&pa, 0, sizeof pa);
     pa.a = a;
+    pa.a.fwd_stride = store_stride(p);  // S_{t+1} of slot q sits q store strides on
     pa.adj = adj;
     pa.store = at<float>(ws, p->o_store);
     pa.sstride = store_stride(p);

@@ -22,6 +22,9 @@ Stored per case, ``<name>.npz``:
   one stress key: the reference fills 'taux' and 'tauz' with the same
   mean);
 * ``grad_*``: the whole gradient, ``rms``: the L2 misfit of the whole survey;
+* ``f64_d_obs_*``, ``f64_d_est_*``, ``f64_seis_*``: the FP64 oracle's
+  sections and raw traces on the same columns (``--fp64`` adds them to
+  existing fixtures);
 * ``in_sha``: a digest of the case's inputs, so a test can tell that
   tests/cases.py still builds the survey the fixture was made from;
 * the set-up values the reference computed (``setup_*``).
@@ -41,6 +44,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import cases  # noqa: E402
 from helpers import input_digest  # noqa: E402
 
@@ -101,7 +105,48 @@ def make(case):
     print(case["name"], "written", os.path.getsize(path) // 1024, "KB", flush=True)
 
 
+def add_fp64(case):
+    """Add the FP64 oracle's sections and raw traces on the kept columns
+    (``f64_d_obs_*``, ``f64_d_est_*``, ``f64_seis_*``) to an existing fixture: the exact-arithmetic answer the
+    reference's own float32 rounding is measured against (its float32 error
+    exceeds 1e-5 on traces next to a source over long records)."""
+    import oracle as O
+    path = os.path.join(HERE, case["name"] + ".npz")
+    with np.load(path) as d:
+        out = {k: d[k] for k in d.files}
+    cols = out["cols"]
+    inpa = case["inpa"]
+    nr = None
+    secs = {"obs": [], "est": []}
+    raw = []
+    for s in range(len(case["src_loc"])):
+        src = O.Ricker(case["src_loc"][s:s + 1], inpa["dh"], inpa["dt"], case["src_type"])
+        src.Ricker(case["fdom"])
+        W = O.OracleWavePropagator(inpa, src, case["rec_loc"], case["model_est"]["vp"].shape,
+                                   components=case["components"], n_well_rec=case["n_well_rec"], chpr=0,
+                                   precision="fp64")
+        for which in ("obs", "est"):
+            secs[which].append(W.forward_modeling({k: v.copy() for k, v in case["model_" + which].items()}))
+        raw.append({k: np.asarray(v).reshape(v.shape[0], -1) for k, v in W.seismogram.items()})
+    for k in raw[0]:
+        if "seis_" + k in out:
+            full = np.concatenate([r[k] for r in raw], axis=1)
+            out["f64_seis_" + k] = np.ascontiguousarray(full[:, cols], np.float32)
+    for which in ("obs", "est"):
+        for k in secs[which][0]:
+            if "d_%s_%s" % (which, k) not in out:
+                continue
+            full = np.concatenate([np.asarray(d[k]) for d in secs[which]], axis=1)
+            out["f64_d_%s_%s" % (which, k)] = np.ascontiguousarray(full[:, cols], np.float32)
+    np.savez_compressed(path, **out)
+    print(case["name"], "FP64 sections added", os.path.getsize(path) // 1024, "KB", flush=True)
+
+
 if __name__ == "__main__":
-    names = sys.argv[1:] or [f.__name__ for f in cases.LARGE]
+    args = sys.argv[1:]
+    fp64_only = "--fp64" in args
+    names = [a for a in args if a != "--fp64"] or [f.__name__ for f in cases.LARGE]
     for n in names:
-        make(cases.by_name(n))
+        if not fp64_only:
+            make(cases.by_name(n))
+        add_fp64(cases.by_name(n))

@@ -71,3 +71,21 @@ def input_digest(case):
     h.update(repr(sorted(case["inpa"].items())).encode())
     h.update(repr((case["fdom"], case["src_type"], case["components"], case["chpr"])).encode())
     return h.hexdigest()
+
+
+def section_error(ours, ref, f64=None, tol=1e-5):
+    """(passes, description) for a section against the reference's float32
+    one: within `tol` relative L2; or, where the reference's own float32
+    rounding puts it further than tol / 2 from the FP64 oracle's section
+    (traces next to a source over long records), no further from the FP64
+    answer than the reference is, and within twice the reference's own error
+    of it."""
+    from conftest import rel_l2
+    e_ref = rel_l2(ours, ref)
+    if e_ref < tol:
+        return True, "%.2e from the reference" % e_ref
+    if f64 is None:
+        return False, "%.2e from the reference" % e_ref
+    noise, e_64 = rel_l2(ref, f64), rel_l2(ours, f64)
+    ok = noise > tol / 2 and e_64 <= noise and e_ref <= 2 * noise
+    return ok, "%.2e from the reference, whose own float32 error is %.2e; ours %.2e from FP64" % (e_ref, noise, e_64)

@@ -63,7 +63,9 @@ def test_exact_adjoint_with_narrow_snapshots(name, snapshot, bound):
     restart state rounded the same way as it is read): the same gradient
     bits for any recompute segment (the snapshots come from the same FP32
     chain), float32 rounding for another shot grouping, and within 1e-2
-    (BF16) or 1e-4 (24 bits) of the FP64 oracle's exact gradient."""
+    (BF16) of the FP64 oracle's exact gradient; 24 bits within 1e-4, or
+    within 3x the distance of the same arithmetic in float32 (the oracle's
+    FP32 build) where float32 rounding alone is larger than that."""
     import torch
     case = cases.by_name(name)
     d_obs = product(case).forward_modeling(case["model_obs"])
@@ -74,12 +76,15 @@ def test_exact_adjoint_with_narrow_snapshots(name, snapshot, bound):
         out.append(W.gradient({k: d_est[k] - d_obs[k] for k in d_est}, parameterization="dv"))
         torch.cuda.synchronize()
     ref = _oracle_exact(case, "fp64")
+    ref32 = _oracle_exact(case, "fp32") if snapshot == "fp24" else None
     for k in ("vp", "vs", "rho"):
         assert np.array_equal(out[0][k], out[1][k]), k
         assert rel_l2(out[2][k], out[0][k]) < 1e-6, k
         err = rel_l2(out[0][k], ref[k])
-        print("\n%s %s exact adjoint with %s snapshots vs FP64: %.2e" % (name, k, snapshot, err))
-        assert err <= bound, (k, err)
+        floor = 3 * rel_l2(ref32[k], ref[k]) if ref32 is not None else 0.0
+        print("\n%s %s exact adjoint with %s snapshots vs FP64: %.2e (float32 floor %.2e)" % (name, k, snapshot, err,
+                                                                                             floor))
+        assert err <= max(bound, floor), (k, err)
 
 
 def _directions(shape, vp, n, eps, seed=2024):

@@ -14,14 +14,17 @@ WavePropagator and its own kernels, run shot by shot on the CPU:
   40-cell water layer (vs = 0), two shots, 1200 samples.
 
 Tolerances (relative L2): seismograms 1e-5 per component on the kept trace
-columns, gradients 1e-4.  The gradient is taken end to end: on the
+columns -- or, where the reference's own float32 rounding is further than
+that from the FP64 oracle (the trace next to a source on the 2000-step
+survey: 2.4e-5), no further from the FP64 answer than the reference is
+(helpers.section_error); gradients 1e-4.  The gradient is taken end to end: on the
 residual of the product's own modelled data, as an FWI iteration would."""
 import numpy as np
 import pytest
 
 import cases
 from conftest import load_golden, rel_l2
-from helpers import l2_residual_np, product
+from helpers import l2_residual_np, product, section_error
 
 pytestmark = pytest.mark.gpu
 
@@ -45,8 +48,9 @@ def _sections_match(d, g, prefix, cols, nt):
             assert k == "tauz" and np.array_equal(v, d["taux"])
             continue
         assert v.shape[0] == nt
-        err = rel_l2(v[:, cols], g[key])
-        assert err < SEIS_TOL, (key, err)
+        ok, why = section_error(v[:, cols], g[key], g.get("f64_" + key), SEIS_TOL)
+        print("\n%s: %s" % (key, why))
+        assert ok, (key, why)
 
 
 def _gradient_matches(grad, g, scale=1.0):
@@ -64,7 +68,7 @@ def _run(name, cols_of=None, widen=1, **extra):
     more shots than the fixture has)."""
     case, g = _case(name)
     if widen > 1:
-        g = {k: (np.concatenate([v] * widen, axis=1) if k.startswith(("d_obs_", "d_est_", "seis_")) else v)
+        g = {k: (np.concatenate([v] * widen, axis=1) if k.startswith(("d_obs_", "d_est_", "seis_", "f64_")) else v)
              for k, v in g.items()}
     if extra.pop("repeat", False):
         case = dict(case, src_loc=np.tile(case["src_loc"], (REPEAT, 1)))
@@ -78,7 +82,8 @@ def _run(name, cols_of=None, widen=1, **extra):
     for k, v in W.seismogram.items():  # (nt, nr, ns) -> the '2d' layout
         v = np.reshape(v, (v.shape[0], -1), order="F")
         if "seis_" + k in g:
-            assert rel_l2(v[:, cols], g["seis_" + k]) < SEIS_TOL, ("seis", k)
+            ok, why = section_error(v[:, cols], g["seis_" + k], g.get("f64_seis_" + k), SEIS_TOL)
+            assert ok, ("seis", k, why)
     res = l2_residual_np(d_est, d_obs)
     res = {k: v for k, v in res.items() if np.any(v)}
     grad = W.gradient(res, parameterization=case["param"])
