@@ -24,8 +24,8 @@ False, or 'auto', the default: on where a launch carries at most 8 M
 cell-shots, where issuing launches from the host would cost a noticeable
 share), ``persist`` (run the time loops as persistent cooperative kernels,
 many steps per launch with a grid barrier between steps, where the layout
-stores every step in FP32 and the tile kernels run: True, False, or 'auto',
-the default: on where a step carries at most 2 M cell-shots),
+stores every step in FP32 and the tile kernels run: True, False (the
+default), or 'auto': on where a step carries at most 2 M cell-shots),
 ``snapshot`` ('fp32'; 'bf16': the forward states the imaging reads are
 stored in BF16 while the forward recurrence stays FP32, halving their memory
 and their reads at the cost of rounding the imaged fields to 8 mantissa bits;
@@ -50,7 +50,12 @@ from .engine import Plan, mean2, smooth
 from .processing import COMPONENTS
 
 FIELDS = COMPONENTS
-DEFAULT_TILE = 0  # step kernel variant when inpa has no 'tile'
+# step kernel variant when inpa has no 'tile': the 16-row tile kernels, or
+# the 8-row ones for surveys of at most SMALL_SURVEY_CELLS cell-shots per step
+# (twice the CTAs per step where a step is a few microseconds of latency:
+# measured on B200, 100 x 100 + 20-cell layer, 4 shots: 8.1 against 11.9 ms
+# per evaluation; 200 x 400 + 20, 10 shots: 108 against 113 ms)
+DEFAULT_TILE, SMALL_TILE, SMALL_SURVEY_CELLS = 0, 1, 8_000_000
 
 
 def _slice_bounds(start, stop, n):
@@ -292,7 +297,7 @@ class WavePreparation:
             o.tile, o.adj_tile = variants
             o.adjoint = N.ADJOINT_EXACT if self.adjoint == "exact" else N.ADJOINT_REFERENCE
             o.graph = int(self._graph_on(inpa.get("graph", "auto"), batch))
-            o.persist = int(self._persist_on(inpa.get("persist", "auto"), batch))
+            o.persist = int(self._persist_on(inpa.get("persist", False), batch))
             o.chunk = int(inpa.get("chunk", 0))
             if chp is not None:
                 o.nchp = int(chp.size)
@@ -310,7 +315,8 @@ class WavePreparation:
                              "'exact' only)")
         snapshot = {"fp32": N.SNAP_FP32, "bf16": N.SNAP_BF16, "fp24": N.SNAP_FP24}[snap]
         self.snapshot = snap
-        tile = inpa.get("tile", DEFAULT_TILE)
+        small = int(self.tnz) * int(self.tnx) * int(self.ns) <= SMALL_SURVEY_CELLS
+        tile = inpa.get("tile", SMALL_TILE if small else DEFAULT_TILE)
         adj_tile = inpa.get("adj_tile", None)
         variants = (0 if tile == "auto" else int(tile), 0 if adj_tile is None else int(adj_tile) + 1)
         seg = int(inpa.get("segment", 0))
@@ -335,8 +341,12 @@ class WavePreparation:
 
     # 'auto' runs the time loops as persistent kernels (many steps per
     # cooperative launch, a grid barrier between steps) where a step carries
-    # at most this many cell-shots: there each step kernel runs for
-    # microseconds and the launches, not the steps, set the pace
+    # at most this many cell-shots.  Off by default: measured on B200 the
+    # grid barrier costs more than the launches it saves (100 x 100 + 20,
+    # 4 shots: 12.4 ms per evaluation persistent, 11.9 one launch per step,
+    # 8.1 with 8-row tiles and graph replay; 200 x 400 + 20, 10 shots: 126
+    # against 113 ms), because a step of a small grid is a few microseconds
+    # of latency that a barrier does not shorten
     PERSIST_AUTO_CELLS = 2_000_000
 
     def _persist_on(self, persist, batch):

@@ -185,8 +185,10 @@ def test_autotuned_variants():
     from pyfwi_b200 import autotune
     case = cases.tiny_chpr()
     g = load_golden("tiny_chpr")
+    from pyfwi_b200 import _native as N
     W = product(case, tile="auto")
-    n = 6
+    n = N.lib().pyfwi_tile_count(int(W.sdo))
+    assert n == 11
     assert 0 <= W.tile < n and 0 <= W.adj_tile < n
     tables = [t for (_, _, t) in autotune._CACHE.values()]
     assert any(sorted(t) == list(range(n)) and all(a > 0 and b > 0 for a, b in t.values()) for t in tables)

@@ -71,11 +71,11 @@ def test_persistent_loops_on_the_200x400_survey():
 
 
 def test_persistent_survey_matches_reference():
-    """The 100 x 100 survey's default ('auto' persists it) against the
-    reference's fixture, on the reference's own residual."""
+    """The 100 x 100 survey with the persistent loops ('auto' persists it)
+    against the reference's fixture, on the reference's own residual."""
     case = cases.c1()
     g = load_golden("c1")
-    W = product(case)
+    W = product(case, persist="auto")
     assert W.plan.opts.persist == 1
     d_est = W.forward_modeling(case["model_est"])
     for k, v in d_est.items():
