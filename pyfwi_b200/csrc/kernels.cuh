@@ -719,11 +719,187 @@ __device__ __forceinline__ void fwd_tile(const StepArgs &a, const V &sv, int bx,
     }
 }
 
-template <int R, int TZ, bool W24>
-__global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ StepArgs a)
+// The step kernels.  fwd_step24 writes 24-bit snapshots through fwd_tile.
+// fwd_step (every other forward step) keeps its own copy of the tile code:
+// measured on B200 the same code reached through fwd_tile ran 3 % slower on
+// the 64-shot survey (the compiler allocates the two differently), so the
+// shared tile function serves the 24-bit, TMA-staged and persistent forms.
+template <int R, int TZ>
+__global__ void __launch_bounds__(NTHREADS) fwd_step24(const __grid_constant__ StepArgs a)
 {
     extern __shared__ float4 smem4[];
-    fwd_tile<R, TZ, W24>(a, a, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<float *>(smem4));
+    fwd_tile<R, TZ, true>(a, a, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<float *>(smem4));
+}
+
+template <int R, int TZ>
+__global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ StepArgs a)
+{
+    using S = FwdShape<R, TZ>;
+    constexpr int SW = S::SW, VW = S::VW, HT = S::HT, HV = S::HV;
+    extern __shared__ float4 smem4[];
+    float *sm = reinterpret_cast<float *>(smem4);
+    float *s_txx = sm, *s_tzz = s_txx + HT * SW, *s_txz = s_tzz + HT * SW;
+    float *s_vx = s_txz + HT * SW, *s_vz = s_vx + HV * VW, *s_b = s_vz + HV * VW;
+    float *s_lam = s_b + HV * VW, *s_mu = s_lam + TZ * TX;  // the tile's cells
+
+    const Grid &g = a.g;
+    const long long P = g.plane;
+    const int slot = blockIdx.z, shot = a.shot0 + slot;
+    const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TZ;
+    const float *in = a.in + slot * a.in_stride;
+    float *out = a.out + slot * a.out_stride;
+    const int tid = threadIdx.x;
+    const float dt = a.k.dt;
+
+    // every copy of the tile in flight at once, then one wait
+    for (int e = tid; e < HT * (SW / 4); e += NTHREADS) {
+        int r = e / (SW / 4), q = e - r * (SW / 4);
+        int gi = i0 - 2 * R + r, gj = j0 - 8 + 4 * q, o = r * SW + 4 * q;
+        cp4(s_txx + o, in + TXX * P, g, gi, gj);
+        cp4(s_tzz + o, in + TZZ * P, g, gi, gj);
+        cp4(s_txz + o, in + TXZ * P, g, gi, gj);
+    }
+    for (int e = tid; e < HV * (VW / 4); e += NTHREADS) {
+        int r = e / (VW / 4), q = e - r * (VW / 4);
+        int gi = i0 - R + r, gj = j0 - 4 + 4 * q, o = r * VW + 4 * q;
+        cp4(s_vx + o, in + VX * P, g, gi, gj);
+        cp4(s_vz + o, in + VZ * P, g, gi, gj);
+        cp4(s_b + o, a.mat + 2 * P, g, gi, gj);
+    }
+    for (int e = tid; e < TZ * (TX / 4); e += NTHREADS) {
+        int r = e / (TX / 4), q = e - r * (TX / 4), o = r * TX + 4 * q;
+        cp4(s_lam + o, a.mat, g, i0 + r, j0 + 4 * q);
+        cp4(s_mu + o, a.mat + P, g, i0 + r, j0 + 4 * q);
+    }
+    cp_wait_all();
+    __syncthreads();
+    if (a.add_src && tid == 0) {  // wave_propagation.py:652-664, elastic_surface.cl:23-28
+        const int si = a.srcz[shot], sj = a.srcx[shot];
+        const int ct = sj - (j0 - 8), cv = sj - (j0 - 4), rt = si - (i0 - 2 * R), rv = si - (i0 - R);
+        if (ct >= 0 && ct < SW && rt >= 0 && rt < HT) {
+            s_txx[rt * SW + ct] += a.src.z;
+            s_tzz[rt * SW + ct] += a.src.w;
+        }
+        if (cv >= 0 && cv < VW && rv >= 0 && rv < HV) {
+            s_vx[rv * VW + cv] += a.src.x;
+            s_vz[rv * VW + cv] += a.src.y;
+        }
+    }
+    __syncthreads();
+
+    // velocities (update_velx / update_velz) on rows i0-R .. and columns
+    // j0-4 .., 4 columns per thread
+    for (int e = tid; e < HV * (VW / 4); e += NTHREADS) {
+        const int r = e / (VW / 4), q = e - r * (VW / 4);
+        const int gi = i0 - R + r, gj = j0 - 4 + 4 * q;
+        const int rt = r + R, ct = 4 * q + 4, o = r * VW + 4 * q;
+        float4 vx = ld4s(s_vx + o), vz = ld4s(s_vz + o);
+        const float4 b = ld4s(s_b + o), dx = damp4(a.dampx, g, gj);
+        const float dz = (gi + ZO >= 0 && gi + ZO < g.rows) ? __ldg(a.dampz + gi + ZO) : 0.f;
+        float t[12];
+        float4 w[2 * R + 1];
+        float rx[4], rz[4];
+        row12(t, s_txx + rt * SW, ct);  // Dx- txx
+#pragma unroll
+        for (int k = 0; k < 4; ++k) rx[k] = xbwd<R>(t, k, a.k.cx);
+        col_rows<R>(w, s_txz, SW, rt, ct);  // Dz- txz
+#pragma unroll
+        for (int k = 0; k < 4; ++k) rz[k] = zbwd<R>(w, k, a.k.cz);
+        float nvx[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float v = f4(vx, k);
+            if (in_domain(g, R, gi, gj + k)) {
+                const float d = f4(dx, k) + dz;
+                v = v + dt * (f4(b, k) * (rx[k] + rz[k]));
+                v = v + dt * (-d * v);
+            }
+            nvx[k] = v;
+        }
+        row12(t, s_txz + rt * SW, ct);  // Dx+ txz
+#pragma unroll
+        for (int k = 0; k < 4; ++k) rx[k] = xfwd<R>(t, k, a.k.cx);
+        col_rows<R>(w, s_tzz, SW, rt, ct);  // Dz+ tzz
+#pragma unroll
+        for (int k = 0; k < 4; ++k) rz[k] = zfwd<R>(w, k, a.k.cz);
+        float nvz[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float v = f4(vz, k);
+            if (in_domain(g, R, gi, gj + k)) {
+                const float d = f4(dx, k) + dz;
+                v = v + dt * (f4(b, k) * (rz[k] + rx[k]));
+                v = v + dt * (-d * v);
+            }
+            nvz[k] = v;
+        }
+        st4s(s_vx + o, make_float4(nvx[0], nvx[1], nvx[2], nvx[3]));
+        st4s(s_vz + o, make_float4(nvz[0], nvz[1], nvz[2], nvz[3]));
+    }
+    __syncthreads();
+
+    // stresses (update_tauz / update_tauxz) on the tile, 4 columns per thread
+    for (int e = tid; e < TZ * (TX / 4); e += NTHREADS) {
+        const int r = e / (TX / 4), q = e - r * (TX / 4);
+        const int gi = i0 + r, gj = j0 + 4 * q;
+        if (gi >= g.tnz || gj >= g.tnx) continue;
+        const int rv = r + R, cv = 4 * q + 4, rt = r + 2 * R, ct = 4 * q + 8;
+        const long long co = cell_off(g, gi, gj);
+        const float4 vxc = ld4s(s_vx + rv * VW + cv), vzc = ld4s(s_vz + rv * VW + cv);
+        float4 txx = ld4s(s_txx + rt * SW + ct), tzz = ld4s(s_tzz + rt * SW + ct), txz = ld4s(s_txz + rt * SW + ct);
+        const float4 lam = ld4s(s_lam + r * TX + 4 * q), mu = ld4s(s_mu + r * TX + 4 * q),
+                     dx = damp4(a.dampx, g, gj);
+        const float dz = __ldg(a.dampz + gi + ZO);
+        float t[12];
+        float4 w[2 * R + 1];
+        float dxp_vx[4], dzm_vz[4], dxm_vz[4], dzp_vx[4];
+        row12(t, s_vx + rv * VW, cv);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dxp_vx[k] = xfwd<R>(t, k, a.k.cx);
+        row12(t, s_vz + rv * VW, cv);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dxm_vz[k] = xbwd<R>(t, k, a.k.cx);
+        col_rows<R>(w, s_vz, VW, rv, cv);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dzm_vz[k] = zbwd<R>(w, k, a.k.cz);
+        col_rows<R>(w, s_vx, VW, rv, cv);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dzp_vx[k] = zfwd<R>(w, k, a.k.cz);
+        float oxx[4], ozz[4], oxz[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float sxx = f4(txx, k), szz = f4(tzz, k), sxz = f4(txz, k);
+            if (in_domain(g, R, gi, gj + k)) {
+                const float l = f4(lam, k), m = f4(mu, k), d = f4(dx, k) + dz;
+                normal_pair_fwd(l, m, dxp_vx[k], dzm_vz[k], d, dt, sxx, szz);
+                sxz = sxz + dt * (m * (dxm_vz[k] + dzp_vx[k]));
+                sxz = sxz + dt * (-d * sxz);
+            }
+            oxx[k] = sxx;
+            ozz[k] = szz;
+            oxz[k] = sxz;
+        }
+        if (gj + 3 < g.tnx) {
+            *reinterpret_cast<float4 *>(out + VX * P + co) = vxc;
+            *reinterpret_cast<float4 *>(out + VZ * P + co) = vzc;
+            *reinterpret_cast<float4 *>(out + TXX * P + co) = make_float4(oxx[0], oxx[1], oxx[2], oxx[3]);
+            *reinterpret_cast<float4 *>(out + TZZ * P + co) = make_float4(ozz[0], ozz[1], ozz[2], ozz[3]);
+            *reinterpret_cast<float4 *>(out + TXZ * P + co) = make_float4(oxz[0], oxz[1], oxz[2], oxz[3]);
+        } else {
+            for (int k = 0; k < 4 && gj + k < g.tnx; ++k) {
+                out[VX * P + co + k] = f4(vxc, k);
+                out[VZ * P + co + k] = f4(vzc, k);
+                out[TXX * P + co + k] = oxx[k];
+                out[TZZ * P + co + k] = ozz[k];
+                out[TXZ * P + co + k] = oxz[k];
+            }
+        }
+        for (int k = 0; k < 4 && gj + k < g.tnx; ++k) {
+            if (a.snap)
+                write_snap(a.snap + slot * a.snap_stride, nullptr, P, co + k, f4(vxc, k), f4(vzc, k), oxx[k], ozz[k], oxz[k]);
+            if (a.rec_row >= 0) record_cell(a, a.rec_row, in, shot, gi, gj + k);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1185,15 +1361,237 @@ __device__ __forceinline__ void adj_tile(const AdjArgs &a, const V &av, int bx, 
     }
 }
 
-// NARROW: the imaging reads BF16 or 24-bit snapshots (fwd16, fwd8) instead
-// of FP32 states.
+// The adjoint step kernels through adj_tile: NS shots per CTA, and (NARROW)
+// the imaging reading BF16 or 24-bit snapshots (fwd16, fwd8) instead of FP32
+// states.
 template <int R, int TZ, bool ENERGY, int NS, bool NARROW>
 __global__ void __launch_bounds__(NTHREADS, AdjOccupancy<R, ENERGY, NS>::value)
-    adj_step(const __grid_constant__ AdjArgs a)
+    adj_step_ns(const __grid_constant__ AdjArgs a)
 {
     extern __shared__ float4 smem4[];
     adj_tile<R, TZ, ENERGY, NS, NARROW, false>(a, a, blockIdx.x, blockIdx.y, blockIdx.z,
                                                reinterpret_cast<float *>(smem4));
+}
+
+__device__ __forceinline__ float bf(const __nv_bfloat16 *p, long long i) { return __bfloat162float(p[i]); }
+
+// adj_step: one shot per CTA, FP32 or BF16 imaged states (the default), with
+// its own copy of the tile code: measured on B200 the same code reached
+// through adj_tile ran 5 % slower on the 64-shot survey.
+template <int R, int TZ, bool ENERGY>
+__global__ void __launch_bounds__(NTHREADS, (R == 2 && !ENERGY) ? 6 : 1) adj_step(const __grid_constant__ AdjArgs a)
+{
+    using S = AdjShape<R, TZ>;
+    constexpr int W = S::W, HT = S::HT, HV = S::HV, VW = TX + 2 * R;
+    extern __shared__ float4 smem4[];
+    float *sm = reinterpret_cast<float *>(smem4);
+    // rows i0-2R ..: b*Avx and b*Avz (the operands of the adjoint stress
+    // differences); after the stress update they hold lam*Atx and
+    // (lam+2mu)*Atz on rows i0-R ..
+    float *s_pvx = sm, *s_pvz = s_pvx + HT * W;
+    // rows i0-R ..: Atx, Atz, Atxz; after the stress update (lam+2mu)*Atx,
+    // lam*Atz, mu*Atxz (the operands of the adjoint velocity differences)
+    float *s_atx = s_pvz + HT * W, *s_atz = s_atx + HV * W, *s_atxz = s_atz + HV * W;
+
+    const Grid &g = a.g;
+    const long long P = g.plane;
+    const int slot = blockIdx.z;
+    const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TZ, sx0 = j0 - 2 * R;
+    const float *in = a.in + slot * a.in_stride;
+    float *out = a.out + slot * a.out_stride;
+    const int tid = threadIdx.x;
+    const float dt = a.k.dt;
+
+    // the stresses as asynchronous copies, in flight while the velocity
+    // products are loaded and stored
+    for (int e = tid; e < HV * (W / 4); e += NTHREADS) {
+        int r = e / (W / 4), q = e - r * (W / 4);
+        int gi = i0 - R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
+        cp4(s_atx + o, in + TXX * P, g, gi, gj);
+        cp4(s_atz + o, in + TZZ * P, g, gi, gj);
+        cp4(s_atxz + o, in + TXZ * P, g, gi, gj);
+    }
+    for (int e = tid; e < HT * (W / 4); e += NTHREADS) {
+        int r = e / (W / 4), q = e - r * (W / 4);
+        int gi = i0 - 2 * R + r, gj = sx0 + 4 * q, o = r * W + 4 * q;
+        const float4 b = ld4(a.mat + 2 * P, g, gi, gj), vx = ld4(in + VX * P, g, gi, gj),
+                     vz = ld4(in + VZ * P, g, gi, gj);
+        st4s(s_pvx + o, make_float4(vx.x * b.x, vx.y * b.y, vx.z * b.z, vx.w * b.w));
+        st4s(s_pvz + o, make_float4(vz.x * b.x, vz.y * b.y, vz.z * b.z, vz.w * b.w));
+    }
+    cp_wait_all();
+    __syncthreads();
+
+    // adjoint stresses on the tile plus an R-cell ring (Adj_update_tau); the
+    // tile's own cells go straight to the output
+    for (int e = tid; e < HV * VW; e += NTHREADS) {
+        int r = e / VW, cc = e - r * VW;
+        int gi = i0 - R + r, gj = j0 - R + cc;
+        int is = r * W + cc + R, iv = is + R * W;
+        const bool tile = r >= R && r < R + TZ && cc >= R && cc < R + TX && gi < g.tnz && gj < g.tnx;
+        float atx = s_atx[is], atz = s_atz[is], atxz = s_atxz[is];
+        if (in_domain(g, R, gi, gj)) {
+            float dx = __ldg(a.dampx + gj + XO), dz = __ldg(a.dampz + gi + ZO);
+            atx = atx + (-dt) * (dx * atx + dfwd<R>(s_pvx, iv, 1, a.k.cx));
+            atz = atz + (-dt) * (dz * atz + dbwd<R>(s_pvz, iv, W, a.k.cz));
+            atxz = atxz + (-dt) * ((dx + dz) * atxz + (dfwd<R>(s_pvx, iv, W, a.k.cz) + dbwd<R>(s_pvz, iv, 1, a.k.cx)));
+            s_atx[is] = atx;
+            s_atz[is] = atz;
+            s_atxz[is] = atxz;
+        }
+        if (tile) {
+            const long long co = cell_off(g, gi, gj);
+            out[TXX * P + co] = atx;
+            out[TZZ * P + co] = atz;
+            out[TXZ * P + co] = atxz;
+        }
+    }
+    __syncthreads();
+
+    // material products of the new adjoint stresses
+    for (int e = tid; e < HV * VW; e += NTHREADS) {
+        int r = e / VW, cc = e - r * VW;
+        int gi = i0 - R + r, gj = j0 - R + cc;
+        int is = r * W + cc + R;
+        // lam = mu = 0 in the zero frame and beyond the allocated rows / columns
+        const bool alloc = gi + ZO >= 0 && gi + ZO < g.rows && gj + XO >= 0 && gj + XO < g.pitch;
+        const long long co = alloc ? cell_off(g, gi, gj) : 0;
+        const float lam = alloc ? __ldg(a.mat + co) : 0.f, mu = alloc ? __ldg(a.mat + P + co) : 0.f;
+        const float l2m = lam + 2.f * mu;
+        const float atx = s_atx[is], atz = s_atz[is], atxz = s_atxz[is];
+        s_atx[is] = l2m * atx;
+        s_atz[is] = lam * atz;
+        s_atxz[is] = mu * atxz;
+        s_pvx[is] = lam * atx;
+        s_pvz[is] = l2m * atz;
+    }
+    __syncthreads();
+
+    // adjoint velocities on the tile (Adj_update_v) and imaging (Grad)
+    const int c = tid % TX;
+    const int gj = j0 + c;
+    if (gj >= g.tnx) return;
+    const int glo = a.npml + R;
+    const float *F = a.fwd ? a.fwd + slot * a.fwd_stride : nullptr;
+    const __nv_bfloat16 *F16 = a.fwd16 ? a.fwd16 + slot * a.fwd_stride : nullptr;
+    float *G = a.gacc + slot * a.gacc_stride;
+    // each thread takes NK consecutive rows of its column, so the z
+    // differences of the imaging slide down register windows (rows gi-R ..
+    // gi+R of the forward vz, tzz and txz): one new row per field and cell
+    constexpr int NK = TZ / (NTHREADS / TX);
+    const int r0 = (tid / TX) * NK;
+    const long long pz = g.pitch;
+    float wvz[2 * R + 1], wtz[2 * R + 1], wtxz[2 * R + 1];
+    const bool win = F && gj >= glo && gj <= g.tnx - R - a.npml && i0 + r0 + NK - 1 >= glo &&
+                     i0 + r0 <= g.tnz - R - a.npml;
+    if (win) {
+        const long long c0 = cell_off(g, i0 + r0, gj);
+#pragma unroll
+        for (int m = 0; m < 2 * R; ++m) {
+            const long long o = c0 + (m - R) * pz;
+            wvz[m + 1] = __ldg(F + VZ * P + o);
+            wtz[m + 1] = __ldg(F + TZZ * P + o);
+            wtxz[m + 1] = __ldg(F + TXZ * P + o);
+        }
+    }
+    for (int k = 0; k < NK; ++k) {
+        const int r = r0 + k, gi = i0 + r;
+        if (gi >= g.tnz) break;
+        int is = (r + R) * W + c + 2 * R;
+        long long co = cell_off(g, gi, gj);
+        if (win) {  // the window moves to rows gi-R .. gi+R
+            const long long o = co + R * pz;
+            shift(wvz, __ldg(F + VZ * P + o));
+            shift(wtz, __ldg(F + TZZ * P + o));
+            shift(wtxz, __ldg(F + TXZ * P + o));
+        }
+        float avx = __ldg(in + VX * P + co), avz = __ldg(in + VZ * P + co);
+        if (in_domain(g, R, gi, gj)) {
+            float dx = __ldg(a.dampx + gj + XO), dz = __ldg(a.dampz + gi + ZO);
+            float sx = dbwd<R>(s_atx, is, 1, a.k.cx) + dbwd<R>(s_atz, is, 1, a.k.cx) + dbwd<R>(s_atxz, is, W, a.k.cz);
+            float sz = dfwd<R>(s_pvx, is, W, a.k.cz) + dfwd<R>(s_pvz, is, W, a.k.cz) + dfwd<R>(s_atxz, is, 1, a.k.cx);
+            avx = avx + (-dt) * ((2.f * dx + dz) * avx + sx);
+            avz = avz + (-dt) * ((dx + 2.f * dz) * avz + sz);
+        }
+        if (!(gi < glo || gi > g.tnz - R - a.npml || gj < glo || gj > g.tnx - R - a.npml)) {
+        const long long sz_ = g.pitch;
+        // the new adjoint stresses this CTA wrote above (plain loads: written in this kernel)
+        const float atx = out[TXX * P + co], atz = out[TZZ * P + co], atxz = out[TXZ * P + co];
+        float dzp_vx, dxm_vz, dxp_vx, dzm_vz, dzp_tz, dxm_tx, dxp_txz, dzm_txz;
+        float vx = 0.f, vz = 0.f, tx = 0.f, tz = 0.f, txz = 0.f;
+        if (F) {
+            // DzpVx is formed from vz, as the reference does (elastic.cl:485)
+            dzp_vx = wfwd<R>(wvz, a.k.cz);
+            dxm_vz = gbwd<R>(F + VZ * P, co, 1, a.k.cx);
+            dxp_vx = gfwd<R>(F + VX * P, co, 1, a.k.cx);
+            dzm_vz = wbwd<R>(wvz, a.k.cz);
+            dzp_tz = wfwd<R>(wtz, a.k.cz);
+            dxm_tx = gbwd<R>(F + TXX * P, co, 1, a.k.cx);
+            dxp_txz = gfwd<R>(F + TXZ * P, co, 1, a.k.cx);
+            dzm_txz = wbwd<R>(wtxz, a.k.cz);
+            if (ENERGY) {
+                vx = F[VX * P + co];
+                vz = wvz[R];
+                tx = F[TXX * P + co];
+                tz = wtz[R];
+                txz = wtxz[R];
+            }
+        } else {
+#define B16F(f, k) bf(F16 + (f) * P, (k))
+#define BFWD(f, s)                                                                                       \
+    (a.k.c##s[0] * (B16F(f, co + st) - B16F(f, co)) + a.k.c##s[1] * (B16F(f, co + 2 * st) - B16F(f, co - st)) + \
+     (R == 4 ? a.k.c##s[2] * (B16F(f, co + 3 * st) - B16F(f, co - 2 * st)) +                              \
+                   a.k.c##s[3] * (B16F(f, co + 4 * st) - B16F(f, co - 3 * st))                            \
+             : 0.f))
+#define BBWD(f, s)                                                                                       \
+    (a.k.c##s[0] * (B16F(f, co) - B16F(f, co - st)) + a.k.c##s[1] * (B16F(f, co + st) - B16F(f, co - 2 * st)) + \
+     (R == 4 ? a.k.c##s[2] * (B16F(f, co + 2 * st) - B16F(f, co - 3 * st)) +                              \
+                   a.k.c##s[3] * (B16F(f, co + 3 * st) - B16F(f, co - 4 * st))                            \
+             : 0.f))
+            long long st = sz_;
+            dzp_vx = BFWD(VZ, z);
+            dzm_vz = BBWD(VZ, z);
+            dzp_tz = BFWD(TZZ, z);
+            dzm_txz = BBWD(TXZ, z);
+            st = 1;
+            dxm_vz = BBWD(VZ, x);
+            dxp_vx = BFWD(VX, x);
+            dxm_tx = BBWD(TXX, x);
+            dxp_txz = BFWD(TXZ, x);
+            if (ENERGY) {
+                vx = B16F(VX, co);
+                vz = B16F(VZ, co);
+                tx = B16F(TXX, co);
+                tz = B16F(TZZ, co);
+                txz = B16F(TXZ, co);
+            }
+#undef B16F
+#undef BFWD
+#undef BBWD
+        }
+        const float b = __ldg(a.mat + 2 * P + co);
+        float gmu = G[0 * P + co], glam = G[1 * P + co], grho = G[2 * P + co];
+        gmu += 2.f * dt * (atx * dxp_vx + atz * dzm_vz) + dt * atxz * (dzp_vx + dxm_vz);
+        glam += dt * (atx + atz) * (dxp_vx + dzm_vz);
+        grho += -(dt * (b * b)) * (avx * (dxm_tx + dzm_txz) + avz * (dzp_tz + dxp_txz));
+        G[0 * P + co] = gmu;
+        G[1 * P + co] = glam;
+        G[2 * P + co] = grho;
+        if (ENERGY) {
+            float dt2 = dt * dt;
+            G[3 * P + co] += 4.f * dt2 * (tx * tx * dxp_vx * dxp_vx + tz * tz * dzm_vz * dzm_vz) +
+                             dt2 * txz * txz * (dzp_vx * dzp_vx + dxm_vz * dxm_vz);
+            G[4 * P + co] += dt2 * (tx * tx + tz * tz) * (dxp_vx * dxp_vx + dzm_vz * dzm_vz);
+            G[5 * P + co] += dt2 * (vx * vx * (dxm_tx * dxm_tx + dzm_txz * dzm_txz) +
+                                    vz * vz * (dzp_tz * dzp_tz + dxp_txz * dxp_txz));
+        }
+        }
+        // the residual the next step injects (Adj_injSrc, elastic_surface.cl:48-71),
+        // added to this step's output after the imaging has read it
+        if (a.epi_row >= 0) inject_epilogue(a, a.epi_row, slot, gi, gj, co, avx, avz, out);
+        out[VX * P + co] = avx;
+        out[VZ * P + co] = avz;
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -174,14 +174,14 @@ int launch_fwd(pyfwi_plan *p, const StepArgs &a, int nslots, cudaStream_t s, boo
         size_t sm = FwdShape<R, TZ>::FLOATS * sizeof(float);
         static bool attr = false;
         if (!attr) {
-            CK(cudaFuncSetAttribute(fwd_step<R, TZ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            CK(cudaFuncSetAttribute(fwd_step<R, TZ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            CK(cudaFuncSetAttribute(fwd_step<R, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            CK(cudaFuncSetAttribute(fwd_step24<R, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
             attr = true;
         }
         if (a.snap8)  // 24-bit snapshots written by their own instance (keeps the others' registers)
-            fwd_step<R, TZ, true><<<grid, NTHREADS, sm, s>>>(a);
+            fwd_step24<R, TZ><<<grid, NTHREADS, sm, s>>>(a);
         else
-            fwd_step<R, TZ, false><<<grid, NTHREADS, sm, s>>>(a);
+            fwd_step<R, TZ><<<grid, NTHREADS, sm, s>>>(a);
     } else {
         size_t sm = RevShape<R, TZ>::FLOATS * sizeof(float);
         static bool attr = false;
@@ -217,15 +217,23 @@ int launch_adj_t(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
     if (rc) return rc;
     dim3 grid((p->g.tnx + TX - 1) / TX, (p->g.tnz + TZ - 1) / TZ, (nslots + NS - 1) / NS);
     size_t sm = adj_smem_floats<R, TZ, E, NS>() * sizeof(float);
+    // one shot per CTA on FP32 or BF16 states: adj_step; else adj_step_ns
+    constexpr bool own = NS == 1 && !NARROW;
     static bool attr = false;
     if (!attr) {
-        CK(cudaFuncSetAttribute(adj_step<R, TZ, E, NS, NARROW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sm));
+        if (own)
+            CK(cudaFuncSetAttribute(adj_step<R, TZ, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        else
+            CK(cudaFuncSetAttribute(adj_step_ns<R, TZ, E, NS, NARROW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sm));
         attr = true;
     }
     AdjArgs b = a;
     b.nslots = nslots;
-    adj_step<R, TZ, E, NS, NARROW><<<grid, NTHREADS, sm, s>>>(b);
+    if (own)
+        adj_step<R, TZ, E><<<grid, NTHREADS, sm, s>>>(b);
+    else
+        adj_step_ns<R, TZ, E, NS, NARROW><<<grid, NTHREADS, sm, s>>>(b);
     p->launches++;
     CKL();
     return PYFWI_OK;
@@ -241,7 +249,7 @@ int launch_adj_ns(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
 template <int R, int TZ>
 int launch_adj(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
 {
-    if (a.fwd16) {  // BF16 / 24-bit snapshots: the 16-row kernel, one shot per CTA (the plan picks no other)
+    if (a.fwd8) {  // 24-bit snapshots: the 16-row kernel, one shot per CTA (the plan picks no other)
         if (TZ != 16 || p->ans != 1) return fail(PYFWI_E_INVALID, "snapshots are imaged by adjoint variant 0 only");
         return p->nacc == 6 ? launch_adj_t<R, 16, true, 1, true>(p, a, nslots, s)
                             : launch_adj_t<R, 16, false, 1, true>(p, a, nslots, s);
