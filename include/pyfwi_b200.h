@@ -122,7 +122,9 @@ typedef struct pyfwi_options {
                                128 / 64 / 256 columns per CTA, 6..7 16-row tile kernels
                                whose adjoint CTAs carry 2 / 4 shots (forward as 0),
                                8..10 tile kernels of 16 / 8 / 32 rows with the forward
-                               tile staged by TMA box copies (adjoint as 0..2) */
+                               tile staged by TMA box copies (adjoint as 0..2), 11 the
+                               16-row tile kernels whose adjoint prefetches the tile's
+                               gradient accumulators into shared memory */
     int32_t graph;          /* 1: replay time loops as CUDA graphs */
     int32_t chunk;          /* streaming kernels: grid rows per CTA, 0 = from the grid size */
     int32_t adj_tile;       /* adjoint+imaging step variant + 1 (same numbering as tile); 0 = tile */

@@ -5,8 +5,9 @@ adjoint+imaging step (``pyfwi_tile_count``): tile kernels with 16, 8 or 32
 rows per tile, TMA-fed streaming kernels 128, 64 or 256 columns wide, and
 16-row tile kernels whose adjoint CTAs carry 2 or 4 shots each (summing
 their imaging in shared memory; their forward step is the first variant's),
-and tile kernels whose forward tile is staged by TMA box copies (their
-adjoint is the cp.async tile kernel's).
+tile kernels whose forward tile is staged by TMA box copies (their
+adjoint is the cp.async tile kernel's), and the tile kernel whose adjoint
+prefetches the tile's gradient accumulators into shared memory.
 Which one is fastest depends on the grid, the number of shots per launch and
 the absorbing layer, so ``tune`` times each on a short record of the survey at
 hand and picks the fastest forward and the fastest adjoint variant

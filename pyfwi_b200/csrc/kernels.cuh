@@ -1378,8 +1378,13 @@ __device__ __forceinline__ float bf(const __nv_bfloat16 *p, long long i) { retur
 // adj_step: one shot per CTA, FP32 or BF16 imaged states (the default), with
 // its own copy of the tile code: measured on B200 the same code reached
 // through adj_tile ran 5 % slower on the 64-shot survey.
-template <int R, int TZ, bool ENERGY>
-__global__ void __launch_bounds__(NTHREADS, (R == 2 && !ENERGY) ? 6 : 1) adj_step(const __grid_constant__ AdjArgs a)
+// PF (variant 11, no energy terms): the tile's three gradient accumulators
+// are copied into shared memory by cp.async at the start, in flight with the
+// stress copies, so the imaging's read-modify-write no longer waits on them
+// in global memory (12 KB more shared memory: 5 CTAs per SM).
+template <int R, int TZ, bool ENERGY, bool PF = false>
+__global__ void __launch_bounds__(NTHREADS, (R == 2 && !ENERGY) ? (PF ? 5 : 6) : 1)
+    adj_step(const __grid_constant__ AdjArgs a)
 {
     using S = AdjShape<R, TZ>;
     constexpr int W = S::W, HT = S::HT, HV = S::HV, VW = TX + 2 * R;
@@ -1401,7 +1406,15 @@ __global__ void __launch_bounds__(NTHREADS, (R == 2 && !ENERGY) ? 6 : 1) adj_ste
     float *out = a.out + slot * a.out_stride;
     const int tid = threadIdx.x;
     const float dt = a.k.dt;
+    float *s_g = s_atxz + HV * W;  // PF: [3][TZ][TX] the tile's accumulators
 
+    if (PF) {  // the accumulators first: their copies wait the longest (DRAM)
+        const float *Gs = a.gacc + slot * a.gacc_stride;
+        for (int e = tid; e < 3 * TZ * (TX / 4); e += NTHREADS) {
+            const int f = e / (TZ * (TX / 4)), rem = e - f * (TZ * (TX / 4)), r = rem / (TX / 4), q = rem - r * (TX / 4);
+            cp4(s_g + (f * TZ + r) * TX + 4 * q, Gs + f * P, g, i0 + r, j0 + 4 * q);
+        }
+    }
     // the stresses as asynchronous copies, in flight while the velocity
     // products are loaded and stored
     for (int e = tid; e < HV * (W / 4); e += NTHREADS) {
@@ -1570,7 +1583,9 @@ __global__ void __launch_bounds__(NTHREADS, (R == 2 && !ENERGY) ? 6 : 1) adj_ste
 #undef BBWD
         }
         const float b = __ldg(a.mat + 2 * P + co);
-        float gmu = G[0 * P + co], glam = G[1 * P + co], grho = G[2 * P + co];
+        float gmu = PF ? s_g[(0 * TZ + r) * TX + c] : G[0 * P + co];
+        float glam = PF ? s_g[(1 * TZ + r) * TX + c] : G[1 * P + co];
+        float grho = PF ? s_g[(2 * TZ + r) * TX + c] : G[2 * P + co];
         gmu += 2.f * dt * (atx * dxp_vx + atz * dzm_vz) + dt * atxz * (dzp_vx + dxm_vz);
         glam += dt * (atx + atz) * (dxp_vx + dzm_vz);
         grho += -(dt * (b * b)) * (avx * (dxm_tx + dzm_txz) + avz * (dzp_tz + dxp_txz));

@@ -67,12 +67,14 @@ size_t up(size_t x, size_t a = ALIGN) { return (x + a - 1) / a * a; }
 // 16-row tile kernels whose adjoint CTAs carry 2 / 4 shots each (the
 // forward step of 6..7 is variant 0's), 8..10 the tile kernels of 16 / 8 /
 // 32 rows with the forward tile staged by TMA box copies (the adjoint of
-// 8..10 is that of 0..2)
-constexpr int TILE_TZ[] = {16, 8, 32, 0, 0, 0, 16, 16, 16, 8, 32};
-constexpr int STREAM_W[] = {0, 0, 0, 128, 64, 256, 0, 0, 0, 0, 0};
-constexpr int ADJ_NS[] = {1, 1, 1, 1, 1, 1, 2, 4, 1, 1, 1};
-constexpr int FWD_TMA[] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1};
-constexpr int N_TILES = 11;
+// 8..10 is that of 0..2), 11 the 16-row tile kernels whose adjoint copies
+// the tile's gradient accumulators into shared memory at its start
+constexpr int TILE_TZ[] = {16, 8, 32, 0, 0, 0, 16, 16, 16, 8, 32, 16};
+constexpr int STREAM_W[] = {0, 0, 0, 128, 64, 256, 0, 0, 0, 0, 0, 0};
+constexpr int ADJ_NS[] = {1, 1, 1, 1, 1, 1, 2, 4, 1, 1, 1, 1};
+constexpr int FWD_TMA[] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 0};
+constexpr int ADJ_PREFETCH[] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1};
+constexpr int N_TILES = 12;
 constexpr int FWD_PF = 4, ADJ_PF = 2;  // rows the streaming kernels fetch ahead
 constexpr size_t ERR_OFF = 128;         // byte offset of the device error word in the header
 constexpr size_t CHECK_OFF = 192;       // byte offset of the frame-check counter (uint64) in the header
@@ -98,7 +100,7 @@ struct pyfwi_plan {
     Grid g;
     Coef k;
     Lines lines;
-    int R, tz, st_w, ftma, atz, ast_w, ans, chunk_opt, nacc, G, ngroups, seg, M, n_inj;  // a*: adjoint step variant
+    int R, tz, st_w, ftma, atz, ast_w, ans, apf, chunk_opt, nacc, G, ngroups, seg, M, n_inj;  // a*: adjoint step variant
     bool exact_adj = false;  // PYFWI_ADJOINT_EXACT
     bool persist = false;    // time loops as persistent kernels (options.persist, where the layout allows)
     int fwd_cap = 0, adj_cap = 0;  // co-resident CTAs of the persistent kernels on this device
@@ -217,20 +219,35 @@ int launch_adj_t(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
     if (rc) return rc;
     dim3 grid((p->g.tnx + TX - 1) / TX, (p->g.tnz + TZ - 1) / TZ, (nslots + NS - 1) / NS);
     size_t sm = adj_smem_floats<R, TZ, E, NS>() * sizeof(float);
-    // one shot per CTA on FP32 or BF16 states: adj_step; else adj_step_ns
+    // one shot per CTA on FP32 or BF16 states: adj_step (with the
+    // accumulators prefetched: variant 11); else adj_step_ns
     constexpr bool own = NS == 1 && !NARROW;
+    const bool pf = own && !E && p->apf;
+    const size_t sm_pf = sm + 3 * TZ * TX * sizeof(float);
     static bool attr = false;
     if (!attr) {
-        if (own)
+        if constexpr (own) {
             CK(cudaFuncSetAttribute(adj_step<R, TZ, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        else
+            if constexpr (!E)
+                CK(cudaFuncSetAttribute(adj_step<R, TZ, E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sm_pf));
+        } else {
             CK(cudaFuncSetAttribute(adj_step_ns<R, TZ, E, NS, NARROW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)sm));
+        }
         attr = true;
     }
     AdjArgs b = a;
     b.nslots = nslots;
-    if (own)
+    if constexpr (own && !E) {
+        if (pf) {
+            adj_step<R, TZ, E, true><<<grid, NTHREADS, sm_pf, s>>>(b);
+            p->launches++;
+            CKL();
+            return PYFWI_OK;
+        }
+    }
+    if constexpr (own)
         adj_step<R, TZ, E><<<grid, NTHREADS, sm, s>>>(b);
     else
         adj_step_ns<R, TZ, E, NS, NARROW><<<grid, NTHREADS, sm, s>>>(b);
@@ -1267,6 +1284,7 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
     p->atz = TILE_TZ[av];
     p->ast_w = STREAM_W[av];
     p->ans = ADJ_NS[av];
+    p->apf = ADJ_PREFETCH[av] && !opt->energy;
     if (opt->snapshot != PYFWI_SNAP_FP32 && opt->checkpoint == PYFWI_CKPT_EXACT) {
         // snapshots are read by the 16-row tile adjoint kernel with one shot per CTA
         p->ast_w = 0;

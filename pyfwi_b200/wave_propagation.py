@@ -13,10 +13,11 @@ torch tensors (outputs stay on the device).
 Extra ``inpa`` keys (all optional): ``checkpoint`` ('exact' or 'reverse';
 default: 'exact' when chpr == 100, else the reference's reverse-time scheme),
 ``segment`` (steps per recompute segment), ``shot_batch``, ``tile`` (step
-kernel variant, 0..10 -- tile kernels of 16 / 8 / 32 rows, streaming kernels
+kernel variant, 0..11 -- tile kernels of 16 / 8 / 32 rows, streaming kernels
 of 128 / 64 / 256 columns, 16-row tile kernels whose adjoint CTAs carry 2 / 4
 shots, tile kernels of 16 / 8 / 32 rows whose forward tile is staged by TMA
-box copies -- or 'auto' to time them all on this survey first and
+box copies, the 16-row tile kernels whose adjoint prefetches its gradient
+accumulators -- or 'auto' to time them all on this survey first and
 take the fastest forward and adjoint variant), ``adj_tile`` (adjoint step
 variant when it differs from ``tile``), ``chunk`` (rows per CTA of the
 streaming variants), ``graph`` (replay whole calls as CUDA graphs: True,

@@ -24,8 +24,8 @@ def _golden_section(g, prefix):
 
 # tile kernel (64 x 16), the streaming kernels (128 / 64 / 256 columns), the
 # tile kernels whose adjoint CTAs carry 2 / 4 shots, the TMA-staged tile
-# forward (64 x 16)
-VARIANTS = [0, 3, 4, 5, 6, 7, 8]
+# forward (64 x 16), the adjoint with prefetched accumulators
+VARIANTS = [0, 3, 4, 5, 6, 7, 8, 11]
 
 
 @pytest.mark.parametrize("tile", VARIANTS)
@@ -134,7 +134,7 @@ def test_tile_variants_agree():
     g = load_golden("tiny_dxr")
     res = l2_residual_np(_golden_section(g, "d_est_"), _golden_section(g, "d_obs_"))
     base = None
-    for tile in range(11):
+    for tile in range(12):
         W = product(case, tile=tile)
         d = W.forward_modeling(case["model_est"])
         gr = W.gradient(res, parameterization=case["param"])
@@ -188,7 +188,7 @@ def test_autotuned_variants():
     from pyfwi_b200 import _native as N
     W = product(case, tile="auto")
     n = N.lib().pyfwi_tile_count(int(W.sdo))
-    assert n == 11
+    assert n == 12
     assert 0 <= W.tile < n and 0 <= W.adj_tile < n
     tables = [t for (_, _, t) in autotune._CACHE.values()]
     assert any(sorted(t) == list(range(n)) and all(a > 0 and b > 0 for a, b in t.values()) for t in tables)
