@@ -134,6 +134,9 @@ typedef struct pyfwi_options {
                                where the layout allows: exact checkpoints holding every step in
                                FP32, the tile kernels (variants 0..2), the reference adjoint;
                                otherwise (and inside a caller's stream capture) one launch per step */
+    int32_t overlap;        /* 1: exact checkpoints in FP32 with recompute segments: recompute
+                               segment m-1 on a second stream of the plan while the adjoint of
+                               segment m runs (two segment buffers in the workspace) */
 } pyfwi_options;
 
 typedef struct pyfwi_plan pyfwi_plan;

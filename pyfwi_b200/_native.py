@@ -37,7 +37,7 @@ REDUCE_SLOTS = 2368  # PYFWI_REDUCE_SLOTS
 class Options(ctypes.Structure):
     _fields_ = [("checkpoint", _i32), ("segment", _i32), ("snapshot", _i32), ("shot_batch", _i32), ("energy", _i32),
                 ("nchp", _i32), ("chp", ctypes.POINTER(_i32)), ("tile", _i32), ("graph", _i32), ("chunk", _i32),
-                ("adj_tile", _i32), ("adjoint", _i32), ("persist", _i32)]
+                ("adj_tile", _i32), ("adjoint", _i32), ("persist", _i32), ("overlap", _i32)]
 
 
 class NativeError(RuntimeError):

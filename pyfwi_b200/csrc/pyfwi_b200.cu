@@ -103,6 +103,9 @@ struct pyfwi_plan {
     int R, tz, st_w, ftma, atz, ast_w, ans, apf, chunk_opt, nacc, G, ngroups, seg, M, n_inj;  // a*: adjoint step variant
     bool exact_adj = false;  // PYFWI_ADJOINT_EXACT
     bool persist = false;    // time loops as persistent kernels (options.persist, where the layout allows)
+    bool overlap = false;    // recompute of segment m-1 on a second stream beside the adjoint of segment m
+    cudaStream_t side = nullptr;          // that second stream (created on first use)
+    std::vector<cudaEvent_t> ovev;        // its events: [2m] recompute of m done, [2m+1] adjoint of m done
     int fwd_cap = 0, adj_cap = 0;  // co-resident CTAs of the persistent kernels on this device
     long long state;  // floats per state (5 planes)
     // workspace offsets in bytes
@@ -557,7 +560,20 @@ bool fp24_snaps(const pyfwi_plan *p) { return bf16_snaps(p) && p->opt.snapshot =
 // S_{(M-1)seg}, then (FP32 snapshots) the seg states of the segment being
 // imaged.  With BF16 snapshots the segment states live in the BF16 store and
 // the FP32 chain that produces them runs in the two work states.
-long long store_stride(const pyfwi_plan *p) { return (long long)(p->M + (bf16_snaps(p) ? 0 : p->seg)) * p->state; }
+// With overlap the segment states take two buffers: segment m uses buffer
+// m % 2, so the recompute of segment m - 1 can fill one while the adjoint of
+// segment m reads the other.
+long long store_stride(const pyfwi_plan *p)
+{
+    return (long long)(p->M + (bf16_snaps(p) ? 0 : p->seg * (p->overlap ? 2 : 1))) * p->state;
+}
+
+// Stored state k (S_{t_lo+k+1}) of segment m, FP32 snapshots.
+Buf seg_state(pyfwi_plan *p, void *ws, int m, int k)
+{
+    const int buf = p->overlap ? (m & 1) : 0;
+    return {at<float>(ws, p->o_store) + (long long)(p->M + buf * p->seg + k) * p->state, store_stride(p)};
+}
 
 // exact mode: where state S_s of the current group lives during a pass
 Buf exact_state(pyfwi_plan *p, void *ws, int s)
@@ -567,8 +583,7 @@ Buf exact_state(pyfwi_plan *p, void *ws, int s)
     long long sstride = store_stride(p);
     if (s == 0) return {store, sstride};
     if (p->M > 1 && s % p->seg == 0 && s / p->seg <= p->M - 1) return {store + (long long)(s / p->seg) * p->state, sstride};
-    if (s > (p->M - 1) * p->seg && !bf16_snaps(p))
-        return {store + (long long)(p->M + s - (p->M - 1) * p->seg - 1) * p->state, sstride};
+    if (s > (p->M - 1) * p->seg && !bf16_snaps(p)) return seg_state(p, ws, p->M - 1, s - (p->M - 1) * p->seg - 1);
     return {work + (long long)(s & 1) * p->state, 2 * p->state};
 }
 
@@ -838,6 +853,72 @@ int adjoint_iter(pyfwi_plan *p, void *ws, AdjArgs &a, int t, int &t_src, int &pi
     return rc;
 }
 
+// Recompute of segment m (steps [t_lo, t_hi)) from its restart state into
+// its segment buffer, on stream `st`.
+int recompute_segment(pyfwi_plan *p, void *ws, int s0, int n, int m, cudaStream_t st)
+{
+    const pyfwi_geometry &G = p->geom;
+    const int t_lo = m * p->seg, t_hi = std::min((m + 1) * p->seg, G.nt);
+    StepArgs f = base_step(p, ws);
+    f.shot0 = s0;
+    Range range("pyfwi recompute segment");
+    for (int t = t_lo; t < t_hi; ++t) {
+        Buf in = t > t_lo ? seg_state(p, ws, m, t - t_lo - 1) : exact_state(p, ws, t), out = seg_state(p, ws, m, t - t_lo);
+        f.in = in.base;
+        f.in_stride = in.stride;
+        f.out = out.base;
+        f.out_stride = out.stride;
+        f.add_src = t % G.dt_scale == 0;
+        f.src = src_at(p, t / G.dt_scale);
+        f.rec_row = -1;
+        int rc = step_fwd(p, f, n, st, false, at<float>(ws, 0));
+        if (rc) return rc;
+    }
+    return PYFWI_OK;
+}
+
+// The exact-checkpoint backward pass of a group with the recompute of
+// segment m - 1 on the plan's second stream while the adjoint of segment m
+// runs on `st`: segment buffers alternate (m % 2); the recompute of m - 1
+// waits for the adjoint of m + 1 to release its buffer, the adjoint of m for
+// the recompute of m.  The results are those of the one-stream schedule.
+int overlap_backward(pyfwi_plan *p, void *ws, AdjArgs &a, int s0, int n, int &t_src, int &ping, float *adj,
+                     cudaStream_t st)
+{
+    const pyfwi_geometry &G = p->geom;
+    if (!p->side) CK(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
+    if ((int)p->ovev.size() < 2 * p->M + 1) {
+        for (int q = (int)p->ovev.size(); q < 2 * p->M + 1; ++q) {
+            cudaEvent_t e;
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            p->ovev.push_back(e);
+        }
+    }
+    cudaEvent_t start = p->ovev[2 * p->M];
+    CK(cudaEventRecord(start, st));  // the side stream starts after everything queued so far
+    CK(cudaStreamWaitEvent(p->side, start, 0));
+    int rc;
+    for (int m = p->M - 1; m >= 0; --m) {
+        const int t_lo = m * p->seg, t_hi = std::min((m + 1) * p->seg, G.nt);
+        if (m >= 1) {  // the recompute of segment m - 1, once the adjoint of m + 1 is done with its buffer
+            if (m + 1 <= p->M - 1) CK(cudaStreamWaitEvent(p->side, p->ovev[2 * (m + 1) + 1], 0));
+            rc = recompute_segment(p, ws, s0, n, m - 1, p->side);
+            if (rc) return rc;
+            CK(cudaEventRecord(p->ovev[2 * (m - 1)], p->side));
+        }
+        if (m < p->M - 1) CK(cudaStreamWaitEvent(st, p->ovev[2 * m], 0));
+        Range range("pyfwi adjoint segment");
+        for (int t = t_hi - 1; t >= std::max(t_lo, 1); --t) {
+            a.fwd = seg_state(p, ws, m, t - t_lo).base;
+            a.fwd_stride = store_stride(p);
+            rc = adjoint_iter(p, ws, a, t, t_src, ping, adj, n, st);
+            if (rc) return rc;
+        }
+        CK(cudaEventRecord(p->ovev[2 * m + 1], st));
+    }
+    return PYFWI_OK;
+}
+
 template <int R, int TZ>
 int launch_exact(pyfwi_plan *p, const ExactArgs &a, int nslots, cudaStream_t s)
 {
@@ -1030,6 +1111,9 @@ int gradient_enqueue(pyfwi_plan *p, void *ws, const float *const *residual, int3
         } else if (p->opt.checkpoint == PYFWI_CKPT_EXACT && use_persist(p, st)) {
             rc = persist_backward(p, ws, a, n, st);  // M == 1: every step stored
             if (rc) return rc;
+        } else if (p->opt.checkpoint == PYFWI_CKPT_EXACT && p->overlap) {
+            rc = overlap_backward(p, ws, a, s0, n, t_src, ping, adj, st);
+            if (rc) return rc;
         } else if (p->opt.checkpoint == PYFWI_CKPT_EXACT) {
             StepArgs f = base_step(p, ws);
             f.shot0 = s0;
@@ -1046,11 +1130,8 @@ int gradient_enqueue(pyfwi_plan *p, void *ws, const float *const *residual, int3
                             f.snap8 = snap8_at(p, ws, t - t_lo);
                             f.snap_stride = (long long)p->seg * p->state;
                         } else {
-                            out = {at<float>(ws, p->o_store) + (long long)(p->M + t - t_lo) * p->state,
-                                   store_stride(p)};
-                            if (t > t_lo)
-                                in = {at<float>(ws, p->o_store) + (long long)(p->M + t - t_lo - 1) * p->state,
-                                      out.stride};
+                            out = seg_state(p, ws, m, t - t_lo);
+                            if (t > t_lo) in = seg_state(p, ws, m, t - t_lo - 1);
                         }
                         f.in = in.base;
                         f.in_stride = in.stride;
@@ -1073,7 +1154,7 @@ int gradient_enqueue(pyfwi_plan *p, void *ws, const float *const *residual, int3
                         a.fwd8 = snap8_at(p, ws, t - t_lo);
                         a.fwd_stride = (long long)p->seg * p->state;
                     } else {
-                        a.fwd = at<float>(ws, p->o_store) + (long long)(p->M + t - t_lo) * p->state;
+                        a.fwd = seg_state(p, ws, m, t - t_lo).base;
                         a.fwd_stride = store_stride(p);
                     }
                     rc = adjoint_iter(p, ws, a, t, t_src, ping, adj, n, st);
@@ -1328,6 +1409,10 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
                  opt->snapshot == PYFWI_SNAP_FP32 && !p->exact_adj && !p->st_w && !p->ftma && !p->ast_w &&
                  p->ans == 1;
     if (p->persist) p->opt.graph = 0;  // a few launches per call: nothing to replay
+    // recompute beside the adjoint: exact checkpoints in FP32 with recompute
+    // segments, the reference adjoint
+    p->overlap = opt->overlap && opt->checkpoint == PYFWI_CKPT_EXACT && p->M > 1 && opt->snapshot == PYFWI_SNAP_FP32 &&
+                 !p->exact_adj;
 
     const size_t pf = (size_t)p->g.plane * sizeof(float), sb = (size_t)p->state * sizeof(float);
     // regions holding planes start on a row of the workspace (a multiple of
@@ -1385,6 +1470,8 @@ int pyfwi_plan_destroy(pyfwi_plan *plan)
         if (plan->ggrad.exec) cudaGraphExecDestroy(plan->ggrad.exec);
         if (plan->gmis.exec) cudaGraphExecDestroy(plan->gmis.exec);
         if (plan->cap) cudaStreamDestroy(plan->cap);
+        for (auto e : plan->ovev) cudaEventDestroy(e);
+        if (plan->side) cudaStreamDestroy(plan->side);
     }
     delete plan;
     return PYFWI_OK;

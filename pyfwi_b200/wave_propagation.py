@@ -27,6 +27,9 @@ share), ``persist`` (run the time loops as persistent cooperative kernels,
 many steps per launch with a grid barrier between steps, where the layout
 stores every step in FP32 and the tile kernels run: True, False (the
 default), or 'auto': on where a step carries at most 2 M cell-shots),
+``overlap`` (exact checkpoints in FP32 with recompute segments: recompute
+segment m - 1 on a second CUDA stream while the adjoint of segment m runs,
+with two segment buffers),
 ``snapshot`` ('fp32'; 'bf16': the forward states the imaging reads are
 stored in BF16 while the forward recurrence stays FP32, halving their memory
 and their reads at the cost of rounding the imaged fields to 8 mantissa bits;
@@ -57,6 +60,9 @@ FIELDS = COMPONENTS
 # measured on B200, 100 x 100 + 20-cell layer, 4 shots: 8.1 against 11.9 ms
 # per evaluation; 200 x 400 + 20, 10 shots: 108 against 113 ms)
 DEFAULT_TILE, SMALL_TILE, SMALL_SURVEY_CELLS = 0, 1, 8_000_000
+# inpa['overlap'] when absent: recompute segment m - 1 on a second stream
+# beside the adjoint of segment m
+OVERLAP_DEFAULT = False
 
 
 def _slice_bounds(start, stop, n):
@@ -299,6 +305,7 @@ class WavePreparation:
             o.adjoint = N.ADJOINT_EXACT if self.adjoint == "exact" else N.ADJOINT_REFERENCE
             o.graph = int(self._graph_on(inpa.get("graph", "auto"), batch))
             o.persist = int(self._persist_on(inpa.get("persist", False), batch))
+            o.overlap = int(bool(inpa.get("overlap", OVERLAP_DEFAULT)))
             o.chunk = int(inpa.get("chunk", 0))
             if chp is not None:
                 o.nchp = int(chp.size)

@@ -97,19 +97,21 @@ def test_configured_survey_matches_reference(name):
     print("\n%s: gradient rel-L2 %s" % (name, {k: "%.1e" % v for k, v in errs.items()}))
 
 
-@pytest.mark.parametrize("tile", [0, 7])
-def test_benchmark_grid_in_its_64_shot_layout(tile):
+@pytest.mark.parametrize("tile,overlap", [(0, False), (7, False), (0, True)])
+def test_benchmark_grid_in_its_64_shot_layout(tile, overlap):
     """The benchmark's grid and launch shape: 64 shots per step launch,
     recompute segments (30 of 40 steps over the 1200-step record), every
     shot a repeat of one of the reference's two; the last two shots checked
     as well as the first two, the gradient against 32 times the
-    reference's; with the one-shot-per-CTA adjoint and with the one whose
-    CTAs carry four shots."""
+    reference's; with the one-shot-per-CTA adjoint, with the one whose CTAs
+    carry four shots, and with the recompute on a second stream beside the
+    adjoint."""
     def cols_of(cols, nr):
         last = (2 * REPEAT - 2) * nr  # shots 62, 63 repeat shots 0, 1
         return np.concatenate([cols, cols + last])
 
-    W, grad, g = _run("c3_parity", cols_of=cols_of, widen=2, repeat=True, shot_batch=64, segment=40, tile=tile)
+    W, grad, g = _run("c3_parity", cols_of=cols_of, widen=2, repeat=True, shot_batch=64, segment=40, tile=tile,
+                       overlap=overlap)
     assert (W.shot_batch, W.segment) == (64, 40), (W.shot_batch, W.segment)
     _gradient_matches(grad, g, scale=REPEAT)
 

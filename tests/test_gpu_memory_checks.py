@@ -43,7 +43,7 @@ def test_no_write_outside_the_domains(name, tile):
 
 @pytest.mark.parametrize("extra", [{"tile": 1}, {"tile": 2}, {"tile": 4}, {"tile": 5}, {"tile": 6}, {"tile": 9}, {"tile": 11},
                                    {"tile": 10}, {"persist": True, "segment": 0, "shot_batch": 0},
-                                   {"snapshot": "fp24", "segment": 7}, {"tile": 0, "adj_tile": 3},
+                                   {"snapshot": "fp24", "segment": 7}, {"overlap": True, "segment": 7}, {"tile": 0, "adj_tile": 3},
                                    {"segment": 7, "shot_batch": 1}, {"snapshot": "bf16", "segment": 9},
                                    {"graph": True}, {"graph": False}])
 def test_no_write_outside_the_domains_variants(extra):

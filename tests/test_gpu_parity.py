@@ -123,6 +123,30 @@ def test_exact_checkpoint_segments_are_bit_identical():
         assert rel_l2(out[2][k], out[0][k]) < 1e-6, k
 
 
+@pytest.mark.parametrize("name,seg,batch", [("tiny_s8", 7, 0), ("tiny_s8", 9, 1), ("c1", 50, 0), ("tiny_dtscale", 11, 0)])
+def test_overlapped_recompute_gives_the_same_bits(name, seg, batch):
+    """inpa['overlap']: the recompute of each segment runs on a second stream
+    beside the adjoint of the segment after it (two segment buffers); the
+    seismograms and gradients are the one-stream schedule's bit for bit."""
+    import torch
+    case = cases.by_name(name)
+    g = load_golden(name)
+    res = l2_residual_np(_golden_section(g, "d_est_"), _golden_section(g, "d_obs_"))
+    res = {k: v for k, v in res.items() if np.any(v)}
+    out = []
+    for overlap in (False, True):
+        W = product(case, segment=seg, shot_batch=batch, overlap=overlap)
+        d = W.forward_modeling(case["model_est"])
+        out.append((d, W.gradient(res, parameterization=case["param"])))
+        torch.cuda.synchronize()
+        assert W.plan.opts.overlap == int(overlap)
+    for a, b in zip(out[0], out[1]):
+        for k in a:
+            assert np.array_equal(a[k], b[k]), (name, k)
+    for k, v in out[1][1].items():
+        assert rel_l2(v, g["grad_" + k]) < GRAD_TOL, k
+
+
 def test_tile_variants_agree():
     """Tile kernels of every height give identical bits (forward and
     gradient); streaming kernels (other FMA grouping) agree to float32
