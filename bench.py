@@ -252,6 +252,8 @@ def run_ours(args, world, rank, local):
         extra["adj_tile"] = args.adj_tile
     if args.overlap is not None:
         extra["overlap"] = bool(args.overlap)
+    if args.snapshot != "fp32":
+        extra["snapshot"] = args.snapshot
     W = product(case, **extra)
     ncell = float(int(W.tnz) * int(W.tnx))
     nint = float((int(W.tnz) - 2 * (int(W.npml) + int(W.sdo)) + 1) * (int(W.tnx) - 2 * (int(W.npml) + int(W.sdo)) + 1))
@@ -323,7 +325,7 @@ def run_ours(args, world, rank, local):
     batched_shots_s = int(W.ns) * args.steps / (ms_max * 1e-3)
     shape = {"ns": int(W.ns), "nt": int(W.nt), "grid": [int(W.tnz), int(W.tnx)]}
     layout = {"checkpoint": W.checkpoint, "segment": W.segment, "shot_batch": W.shot_batch,
-              "overlap": int(W.plan.opts.overlap),
+              "overlap": int(W.plan.opts.overlap), "snapshot": W.snapshot,
               "kernels": {"forward": int(W.tile), "adjoint": int(W.adj_tile)}}
     plain = None
     if world == 1 and (args.plain_shots > 0 or args.inversion > 0 or args.uneven > 0 or args.configs):
@@ -606,6 +608,8 @@ def main():
     ap.add_argument("--segment", type=int, default=0, help="steps per recompute segment (default: auto)")
     ap.add_argument("--tile", default=None, help="step kernel variant 0..5, or 'auto' (autotuner)")
     ap.add_argument("--adj-tile", type=int, default=None, help="adjoint step kernel variant when it differs")
+    ap.add_argument("--snapshot", choices=["fp32", "fp24", "bf16"], default="fp32",
+                    help="format of the imaged forward states (fp24: within the gradient bar at 3/4 of the store)")
     ap.add_argument("--overlap", type=int, default=None,
                     help="1: recompute segments on a second stream beside the adjoint (default: the library's)")
     ap.add_argument("--plain-shots", type=int, default=2,
