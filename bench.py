@@ -42,7 +42,10 @@ WORKLOAD = "elastic FWI gradient, 500x1000 cells (+30-cell absorbing layer), 64 
 # algorithmic bytes per cell and shot-step (one FP32 read or write = 4 B)
 BYTES_FWD = 52.0         # read vx vz txx tzz txz lam mu b, write 5 fields
 BYTES_ADJ = 52.0         # adjoint propagation: same count
-BYTES_IMG = 44.0         # imaging: read 5 forward fields, read+write 3 gradients
+# imaging, per imaged cell: read 5 values of the forward state or of its
+# difference set (4, 3 or 2 B each: FP32, 24-bit, BF16), read and write 3
+# gradients (24 B); the forward steps that fill difference sets write 5
+# values per imaged cell once per shot-step
 
 
 def peaks():
@@ -254,6 +257,8 @@ def run_ours(args, world, rank, local):
         extra["overlap"] = bool(args.overlap)
     if args.snapshot != "fp32":
         extra["snapshot"] = args.snapshot
+    if args.store is not None:
+        extra["store"] = args.store
     W = product(case, **extra)
     ncell = float(int(W.tnz) * int(W.tnx))
     nint = float((int(W.tnz) - 2 * (int(W.npml) + int(W.sdo)) + 1) * (int(W.tnx) - 2 * (int(W.npml) + int(W.sdo)) + 1))
@@ -324,8 +329,10 @@ def run_ours(args, world, rank, local):
     misfit = float(rms.item())
     batched_shots_s = int(W.ns) * args.steps / (ms_max * 1e-3)
     shape = {"ns": int(W.ns), "nt": int(W.nt), "grid": [int(W.tnz), int(W.tnx)]}
+    W_store_diffs, W_snapshot = W.plan.store_diffs, W.snapshot
     layout = {"checkpoint": W.checkpoint, "segment": W.segment, "shot_batch": W.shot_batch,
               "overlap": int(W.plan.opts.overlap), "snapshot": W.snapshot,
+              "store": "differences" if W_store_diffs else "states",
               "kernels": {"forward": int(W.tile), "adjoint": int(W.adj_tile)}}
     plain = None
     if world == 1 and (args.plain_shots > 0 or args.inversion > 0 or args.uneven > 0 or args.configs):
@@ -335,32 +342,47 @@ def run_ours(args, world, rank, local):
     if world == 1 and args.plain_shots > 0:
         plain = plain_form(args, dev, batched_shots_s)
     hbm, peak_src = peaks()
+    store = "differences" if W_store_diffs else "states"
+    # bytes per value of what the imaging reads: FP32 states or difference
+    # sets, 24-bit (BF16 + byte) or BF16 snapshots
+    vb = {"fp32": 4.0, "fp24": 3.0, "bf16": 2.0}[W_snapshot]
+    # difference sets: every shot-step's set written once, by the forward
+    # step that produces (or reads) that state, over the imaged cells
+    q_bytes = 5 * vb * nint * int(shape["ns"]) * int(shape["nt"]) * args.steps if store == "differences" else 0.0
+
+    def kernel_roof(k):
+        n_l, ms_k, cells_k = prof[k]
+        if k == 1:  # propagation + imaging (interior cells: 5 imaged values, 3 gradients read and written)
+            alg = cells_k * BYTES_ADJ + (cells_k / ncell) * nint * (5 * vb + 24.0)
+        else:
+            alg = cells_k * BYTES_FWD + (q_bytes if k == 0 else 0.0)
+        ach = alg / (ms_k * 1e-3) / 1e9 if ms_k > 0 else None
+        return {"achieved": ach, "frac": ach / hbm if ach else None, "launches": n_l,
+                "avg_launch_ms": ms_k / max(n_l, 1), "alg_bytes_per_launch": alg / max(n_l, 1)}
+
+    names = {0: "fwd_step", 1: "adj_step", 2: "rev_step"}
+    per_kernel = {names[k]: kernel_roof(k) for k in prof if prof[k][0] > 0}
     # dominant kernel: the one with the most device time
-    kinds = {0: ("fwd_step", BYTES_FWD), 1: ("adj_step", None), 2: ("rev_step", BYTES_FWD)}
     dom = max(prof, key=lambda k: prof[k][1])
-    n_l, ms_k, cells_k = prof[dom]
-    name, bpc = kinds[dom]
-    if dom == 1:
-        alg_bytes = cells_k * BYTES_ADJ + (cells_k / ncell) * nint * BYTES_IMG
-    else:
-        alg_bytes = cells_k * bpc
-    achieved = alg_bytes / (ms_k * 1e-3) / 1e9 if ms_k > 0 else None
+    name = names[dom]
+    kr = per_kernel[name]
     traffic, traffic_src = None, None
     tp = os.path.join(ROOT, "profiles", "traffic_%s_c3.json" % name)
     if os.path.exists(tp) and args.config == "c3":
         with open(tp) as f:
             tj = json.load(f)
-        # ncu DRAM bytes per cell-shot of one launch of the profile's capture,
-        # times the cell-shots of this run's average launch
-        traffic = tj["dram_bytes_per_cell_shot"] * cells_k / max(n_l, 1)
-        traffic_src = {"ncu_capture": tj.get("capture"), "shots_per_launch": tj.get("shots_per_launch"),
-                       "scaled_to": "cell-shots of this run's average launch"}
-    roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm if achieved else None, "traffic": traffic, "traffic_source": traffic_src,
-            "peak_source": peak_src,
-            "launches": n_l, "avg_launch_ms": ms_k / max(n_l, 1),
-            "alg_bytes_per_launch": alg_bytes / max(n_l, 1),
-            "kernel_share": {kinds[k][0]: prof[k][1] / max(ms, 1e-9) for k in prof}}
+        if tj.get("store", "states") == store and tj.get("snapshot", "fp32") == W_snapshot:
+            # ncu DRAM bytes per cell-shot of one launch of the profile's
+            # capture, times the cell-shots of this run's average launch
+            traffic = tj["dram_bytes_per_cell_shot"] * prof[dom][2] / max(prof[dom][0], 1)
+            traffic_src = {"ncu_capture": tj.get("capture"), "shots_per_launch": tj.get("shots_per_launch"),
+                           "scaled_to": "cell-shots of this run's average launch"}
+    roof = {"bound": "hbm", "kernel": name, "achieved": kr["achieved"], "peak": hbm, "unit": "GB/s",
+            "frac": kr["frac"], "traffic": traffic, "traffic_source": traffic_src, "peak_source": peak_src,
+            "launches": kr["launches"], "avg_launch_ms": kr["avg_launch_ms"],
+            "alg_bytes_per_launch": kr["alg_bytes_per_launch"],
+            "kernel_share": {names[k]: prof[k][1] / max(ms, 1e-9) for k in prof},
+            "per_kernel": per_kernel}
     small = None
     if world == 1 and args.configs:
         gc.collect()
@@ -518,7 +540,7 @@ def configs_run(args, dev):
     for name in ("c1", "c2"):
         case = cases.by_name(name)
         gpu = {}
-        forms = (("plain", {"graph": False, "persist": False, "shot_batch": 1, "segment": 0}),
+        forms = (("plain", {"graph": False, "persist": False, "shot_batch": 1, "segment": 0, "store": "states"}),
                  ("launches", {"graph": False, "persist": False}), ("graph", {"graph": True, "persist": False}),
                  ("persistent", {"persist": True, "shot_batch": 0, "segment": 0}))
         for form, extra in forms:
@@ -562,7 +584,8 @@ def plain_form(args, dev, batched_shots_s):
     import torch
     from helpers import product
     case = survey(args.plain_shots, args.nt)
-    extra = {"cuda_device": str(dev), "segment": 0, "shot_batch": 1, "graph": False, "persist": False}
+    extra = {"cuda_device": str(dev), "segment": 0, "shot_batch": 1, "graph": False, "persist": False,
+             "store": "states"}
     if args.tile is not None:
         extra["tile"] = args.tile if args.tile == "auto" else int(args.tile)
     if args.adj_tile is not None:
@@ -610,6 +633,8 @@ def main():
     ap.add_argument("--adj-tile", type=int, default=None, help="adjoint step kernel variant when it differs")
     ap.add_argument("--snapshot", choices=["fp32", "fp24", "bf16"], default="fp32",
                     help="format of the imaged forward states (fp24: within the gradient bar at 3/4 of the store)")
+    ap.add_argument("--store", choices=["differences", "states"], default=None,
+                    help="what the checkpoint segments hold for the imaging (default: the library's)")
     ap.add_argument("--overlap", type=int, default=None,
                     help="1: recompute segments on a second stream beside the adjoint (default: the library's)")
     ap.add_argument("--plain-shots", type=int, default=2,

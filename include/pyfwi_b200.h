@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PYFWI_ABI_VERSION 7
+#define PYFWI_ABI_VERSION 8
 
 enum pyfwi_status {
     PYFWI_OK = 0,
@@ -137,6 +137,13 @@ typedef struct pyfwi_options {
     int32_t overlap;        /* 1: exact checkpoints in FP32 with recompute segments: recompute
                                segment m-1 on a second stream of the plan while the adjoint of
                                segment m runs (two segment buffers in the workspace) */
+    int32_t store_diffs;    /* 1: exact checkpoints in FP32, reference adjoint without energy
+                               terms, tile kernels 0..2: the forward steps that fill the segment
+                               store write the five differences of each state that the imaging
+                               reads (Dx+ vx, Dz- vz, Dz+ vz + Dx- vz, Dx- txx + Dz- txz,
+                               Dz+ tzz + Dx+ txz) in place of the state, and the adjoint step
+                               reads them instead of differencing the state; the recurrence
+                               runs in the two work states.  Same store size; otherwise ignored */
 } pyfwi_options;
 
 typedef struct pyfwi_plan pyfwi_plan;
@@ -257,6 +264,12 @@ int pyfwi_tile_count(int32_t half_order);
 
 /* Kernel launches this plan issued since creation (for launch accounting). */
 int pyfwi_launch_count(const pyfwi_plan *plan, int64_t *count);
+
+/* What the plan made of the options that apply only where its layout
+ * allows: *flags bit 0 persistent time loops (options.persist), bit 1
+ * recompute beside the adjoint (options.overlap), bit 2 difference sets in the
+ * checkpoint segments (options.store_diffs).  No reference counterpart. */
+int pyfwi_plan_flags(const pyfwi_plan *plan, int32_t *flags);
 
 /* Read and clear the workspace's device error word after the work queued on
  * `stream` (synchronises that stream).  *code: 0 none, 1 a streaming kernel

@@ -30,14 +30,15 @@ class Geometry(ctypes.Structure):
                 ("mask_row0", _i32), ("mask_row1", _i32), ("mask_col0", _i32), ("mask_col1", _i32)]
 
 
-ABI_VERSION = 7  # PYFWI_ABI_VERSION of include/pyfwi_b200.h
+ABI_VERSION = 8  # PYFWI_ABI_VERSION of include/pyfwi_b200.h
 REDUCE_SLOTS = 2368  # PYFWI_REDUCE_SLOTS
 
 
 class Options(ctypes.Structure):
     _fields_ = [("checkpoint", _i32), ("segment", _i32), ("snapshot", _i32), ("shot_batch", _i32), ("energy", _i32),
                 ("nchp", _i32), ("chp", ctypes.POINTER(_i32)), ("tile", _i32), ("graph", _i32), ("chunk", _i32),
-                ("adj_tile", _i32), ("adjoint", _i32), ("persist", _i32), ("overlap", _i32)]
+                ("adj_tile", _i32), ("adjoint", _i32), ("persist", _i32), ("overlap", _i32),
+                ("store_diffs", _i32)]
 
 
 class NativeError(RuntimeError):
@@ -71,6 +72,7 @@ def lib():
     L.pyfwi_smooth.argtypes = [_P, _P, _P, _i32, _i32, _i32, ctypes.POINTER(ctypes.c_double), _i32, _P]
     L.pyfwi_tile_count.argtypes = [_i32]
     L.pyfwi_launch_count.argtypes = [_P, ctypes.POINTER(ctypes.c_int64)]
+    L.pyfwi_plan_flags.argtypes = [_P, ctypes.POINTER(_i32)]
     L.pyfwi_device_error.argtypes = [_P, _P, ctypes.c_size_t, ctypes.POINTER(_i32), _P]
     L.pyfwi_wait_selftest.argtypes = [_P, _P, ctypes.c_size_t, ctypes.c_int64, _P]
     L.pyfwi_barrier_selftest.argtypes = [_P, _P, ctypes.c_size_t, ctypes.c_int64, _P]
@@ -86,7 +88,7 @@ def lib():
                           "`python -m pyfwi_b200.build`" % (L.pyfwi_abi_version(), ABI_VERSION))
     for name in ("pyfwi_plan_create", "pyfwi_plan_destroy", "pyfwi_workspace_size", "pyfwi_set_model",
                  "pyfwi_forward", "pyfwi_gradient", "pyfwi_l2_residual", "pyfwi_mean2", "pyfwi_tile_count",
-                 "pyfwi_launch_count", "pyfwi_profile_enable", "pyfwi_profile_read", "pyfwi_device_error",
+                 "pyfwi_launch_count", "pyfwi_plan_flags", "pyfwi_profile_enable", "pyfwi_profile_read", "pyfwi_device_error",
                  "pyfwi_smooth", "pyfwi_misfit_gradient", "pyfwi_lowpass", "pyfwi_wait_selftest", "pyfwi_barrier_selftest",
                  "pyfwi_frame_check", "pyfwi_checkpoint_states"):
         getattr(L, name).restype = ctypes.c_int

@@ -321,7 +321,29 @@ struct StepArgs {
     long long snap_stride; // elements between the snapshots of consecutive slots
     const float *tbase;    // streaming kernels: workspace base = row 0 of `tmap`
     int *err;              // streaming kernels: workspace error word
+    // nullable: the imaging's differences of the output state (planes
+    // Q_DXP_VX, Q_DZM_VZ, Q_VZS), and of the input state (planes Q_TXS,
+    // Q_TZS), slot 0; written by fwd_step<R, TZ, QD>: FP32 planes (QD 1), or
+    // BF16 planes of the upper 16 bits with byte planes qout8 / qin8 of the
+    // next 8 (QD 2, 24-bit values)
+    void *qout;
+    void *qin;
+    unsigned char *qout8, *qin8;
+    long long q_stride;    // elements between the difference sets of consecutive slots
+    int qlo, qhi_z, qhi_x; // the imaged cells: rows qlo .. qhi_z, columns qlo .. qhi_x (the only ones written)
     alignas(64) CUtensorMap tmap;  // streaming kernels: the workspace as rows of `pitch` floats
+};
+
+// The imaging's differences of a forward state S (elastic.cl:470-526), the
+// five planes a difference set holds in place of S when the plan stores
+// differences: what the zero-lag imaging of the adjoint step reads instead of
+// differencing S itself.  The sums are those the imaging forms, in its order.
+enum {
+    Q_DXP_VX = 0,  // Dx+ vx
+    Q_DZM_VZ = 1,  // Dz- vz
+    Q_VZS = 2,     // Dz+ vz + Dx- vz  (the reference forms DzpVx from vz, elastic.cl:485)
+    Q_TXS = 3,     // Dx- txx + Dz- txz
+    Q_TZS = 4      // Dz+ tzz + Dx+ txz
 };
 
 // Snapshot of the five fields written at cell `co` (round to nearest even):
@@ -441,6 +463,54 @@ struct FwdShape {
 
 __device__ __forceinline__ float4 ld4s(const float *s) { return *reinterpret_cast<const float4 *>(s); }
 __device__ __forceinline__ float f4(const float4 &v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+
+// Difference planes: four values of one row from element o (a multiple of
+// 4), or one value, as FP32 (QD 1) or 24 bits (QD 2: the upper 16 bits of
+// the value rounded to nearest even at 15 mantissa bits in a BF16 plane q,
+// the next 8 in a byte plane q8).
+template <int QD>
+__device__ __forceinline__ void qst4(void *q, unsigned char *q8, long long o, float4 v)
+{
+    if constexpr (QD == 1) {
+        *reinterpret_cast<float4 *>(static_cast<float *>(q) + o) = v;
+    } else {
+        const unsigned b0 = fp24_bits(v.x), b1 = fp24_bits(v.y), b2 = fp24_bits(v.z), b3 = fp24_bits(v.w);
+        *reinterpret_cast<uint2 *>(static_cast<__nv_bfloat16 *>(q) + o) =
+            make_uint2((b0 >> 8) | ((b1 >> 8) << 16), (b2 >> 8) | ((b3 >> 8) << 16));
+        *reinterpret_cast<unsigned *>(q8 + o) = (b0 & 0xFFu) | ((b1 & 0xFFu) << 8) | ((b2 & 0xFFu) << 16) | (b3 << 24);
+    }
+}
+
+template <int QD>
+__device__ __forceinline__ float qld(const float *F, const __nv_bfloat16 *F16, const unsigned char *F8, long long o)
+{
+    if constexpr (QD == 1) {
+        return __ldg(F + o);
+    } else {
+        const unsigned hi = __ldg(reinterpret_cast<const unsigned short *>(F16) + o), lo = __ldg(F8 + o);
+        return __uint_as_float((hi << 16) | (lo << 8));
+    }
+}
+
+template <int QD>
+__device__ __forceinline__ void qst1(void *q, unsigned char *q8, long long o, float v)
+{
+    if constexpr (QD == 1)
+        static_cast<float *>(q)[o] = v;
+    else
+        write_snap1(static_cast<__nv_bfloat16 *>(q), q8, o, v);
+}
+
+// Four values of one row from cell co (column gj) on: one float4 store when
+// the four columns are inside the grid, else one store per column.
+__device__ __forceinline__ void st4row(float *plane, long long co, int gj, int tnx, float4 v)
+{
+    if (gj + 3 < tnx) {
+        *reinterpret_cast<float4 *>(plane + co) = v;
+    } else {
+        for (int k = 0; k < 4 && gj + k < tnx; ++k) plane[co + k] = f4(v, k);
+    }
+}
 
 // Three aligned float4 of a shared row around column c (c - 4 .. c + 7).
 __device__ __forceinline__ void row12(float (&v)[12], const float *row, int c)
@@ -731,8 +801,14 @@ __global__ void __launch_bounds__(NTHREADS) fwd_step24(const __grid_constant__ S
     fwd_tile<R, TZ, true>(a, a, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<float *>(smem4));
 }
 
-template <int R, int TZ>
-__global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ StepArgs a)
+// QD (1: FP32, 2: 24 bits): the step also writes the imaging's differences
+// of its output state (a.qout: velocity planes) and of its input state
+// (a.qin, nullable: stress planes) for the adjoint to read in place of the
+// stored state; four more floats of shared memory (the input stresses at the
+// source cell before this step's source is added), at most 64 registers
+// (4 CTAs per SM) at half order 2.
+template <int R, int TZ, int QD = 0>
+__global__ void __launch_bounds__(NTHREADS, QD ? (R == 2 ? 4 : 2) : 0) fwd_step(const __grid_constant__ StepArgs a)
 {
     using S = FwdShape<R, TZ>;
     constexpr int SW = S::SW, VW = S::VW, HT = S::HT, HV = S::HV;
@@ -777,6 +853,10 @@ __global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ Ste
         const int si = a.srcz[shot], sj = a.srcx[shot];
         const int ct = sj - (j0 - 8), cv = sj - (j0 - 4), rt = si - (i0 - 2 * R), rv = si - (i0 - R);
         if (ct >= 0 && ct < SW && rt >= 0 && rt < HT) {
+            if constexpr (QD) {  // the stored input state has no source of this step
+                s_mu[TZ * TX] = s_txx[rt * SW + ct];
+                s_mu[TZ * TX + 1] = s_tzz[rt * SW + ct];
+            }
             s_txx[rt * SW + ct] += a.src.z;
             s_tzz[rt * SW + ct] += a.src.w;
         }
@@ -816,6 +896,13 @@ __global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ Ste
             }
             nvx[k] = v;
         }
+        const bool qtile = QD && a.qin && r >= R && r < R + TZ && q >= 1 && q <= TX / 4 && gi >= a.qlo &&
+                           gi <= a.qhi_z && gj + 3 >= a.qlo && gj <= a.qhi_x;
+        if constexpr (QD) {
+            if (qtile)
+                qst4<QD>(a.qin, a.qin8, slot * a.q_stride + Q_TXS * P + cell_off(g, gi, gj),
+                         make_float4(rx[0] + rz[0], rx[1] + rz[1], rx[2] + rz[2], rx[3] + rz[3]));
+        }
         row12(t, s_txz + rt * SW, ct);  // Dx+ txz
 #pragma unroll
         for (int k = 0; k < 4; ++k) rx[k] = xfwd<R>(t, k, a.k.cx);
@@ -833,10 +920,44 @@ __global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ Ste
             }
             nvz[k] = v;
         }
+        if constexpr (QD) {
+            if (qtile)
+                qst4<QD>(a.qin, a.qin8, slot * a.q_stride + Q_TZS * P + cell_off(g, gi, gj),
+                         make_float4(rz[0] + rx[0], rz[1] + rx[1], rz[2] + rx[2], rz[3] + rx[3]));
+        }
         st4s(s_vx + o, make_float4(nvx[0], nvx[1], nvx[2], nvx[3]));
         st4s(s_vz + o, make_float4(nvz[0], nvz[1], nvz[2], nvz[3]));
     }
     __syncthreads();
+    if constexpr (QD) {
+        // The stress differences above saw this step's source at its cell;
+        // the imaging wants those of the stored input state: thread 0
+        // recomputes the cells whose stencils reach the source cell (row si,
+        // columns sj-R+1 .. sj+R for Dx- txx; column sj, rows si-R .. si+R-1
+        // for Dz+ tzz) with the values from before the source was added, and
+        // overwrites them (ordered after the loop's stores by the barrier).
+        if (a.qin && a.add_src && tid == 0) {
+            const int si = a.srcz[shot], sj = a.srcx[shot];
+            const int rt = si - (i0 - 2 * R), ct = sj - (j0 - 8);
+            if (ct >= 0 && ct < SW && rt >= 0 && rt < HT) {
+                const long long src = (long long)rt * SW + ct;
+                const float oxx = s_mu[TZ * TX], ozz = s_mu[TZ * TX + 1];
+                auto lxx = [&](long long k) { return k == src ? oxx : s_txx[k]; };
+                auto lzz = [&](long long k) { return k == src ? ozz : s_tzz[k]; };
+                auto lxz = [&](long long k) { return s_txz[k]; };
+                const long long qo = slot * a.q_stride;
+                for (int m = 0; m < 4 * R; ++m) {
+                    const int gi = m < 2 * R ? si : si - R + (m - 2 * R);
+                    const int gj = m < 2 * R ? sj - R + 1 + m : sj;
+                    if (gi < i0 || gi >= i0 + TZ || gj < j0 || gj >= j0 + TX || gi >= g.tnz || gj >= g.tnx) continue;
+                    const long long c = (long long)(gi - (i0 - 2 * R)) * SW + (gj - (j0 - 8));
+                    const long long co = cell_off(g, gi, gj);
+                    qst1<QD>(a.qin, a.qin8, qo + Q_TXS * P + co, lbwd<R>(lxx, c, 1, a.k.cx) + lbwd<R>(lxz, c, SW, a.k.cz));
+                    qst1<QD>(a.qin, a.qin8, qo + Q_TZS * P + co, lfwd<R>(lzz, c, SW, a.k.cz) + lfwd<R>(lxz, c, 1, a.k.cx));
+                }
+            }
+        }
+    }
 
     // stresses (update_tauz / update_tauxz) on the tile, 4 columns per thread
     for (int e = tid; e < TZ * (TX / 4); e += NTHREADS) {
@@ -859,6 +980,15 @@ __global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ Ste
         row12(t, s_vz + rv * VW, cv);
 #pragma unroll
         for (int k = 0; k < 4; ++k) dxm_vz[k] = xbwd<R>(t, k, a.k.cx);
+        if constexpr (QD) {  // Dz+ vz + Dx- vz of the output state, from scalar shared loads
+            if (a.qout && gi >= a.qlo && gi <= a.qhi_z && gj + 3 >= a.qlo && gj <= a.qhi_x) {
+                const int iv = rv * VW + cv;
+                qst4<QD>(a.qout, a.qout8, slot * a.q_stride + Q_VZS * P + co,
+                     make_float4(dfwd<R>(s_vz, iv, VW, a.k.cz) + dxm_vz[0], dfwd<R>(s_vz, iv + 1, VW, a.k.cz) + dxm_vz[1],
+                                 dfwd<R>(s_vz, iv + 2, VW, a.k.cz) + dxm_vz[2],
+                                 dfwd<R>(s_vz, iv + 3, VW, a.k.cz) + dxm_vz[3]));
+            }
+        }
         col_rows<R>(w, s_vz, VW, rv, cv);
 #pragma unroll
         for (int k = 0; k < 4; ++k) dzm_vz[k] = zbwd<R>(w, k, a.k.cz);
@@ -878,6 +1008,13 @@ __global__ void __launch_bounds__(NTHREADS) fwd_step(const __grid_constant__ Ste
             oxx[k] = sxx;
             ozz[k] = szz;
             oxz[k] = sxz;
+        }
+        if constexpr (QD) {  // the velocity differences of the output state
+            if (a.qout && gi >= a.qlo && gi <= a.qhi_z && gj + 3 >= a.qlo && gj <= a.qhi_x) {
+                const long long qo = slot * a.q_stride + co;
+                qst4<QD>(a.qout, a.qout8, qo + Q_DXP_VX * P, make_float4(dxp_vx[0], dxp_vx[1], dxp_vx[2], dxp_vx[3]));
+                qst4<QD>(a.qout, a.qout8, qo + Q_DZM_VZ * P, make_float4(dzm_vz[0], dzm_vz[1], dzm_vz[2], dzm_vz[3]));
+            }
         }
         if (gj + 3 < g.tnx) {
             *reinterpret_cast<float4 *>(out + VX * P + co) = vxc;
@@ -1382,7 +1519,12 @@ __device__ __forceinline__ float bf(const __nv_bfloat16 *p, long long i) { retur
 // are copied into shared memory by cp.async at the start, in flight with the
 // stress copies, so the imaging's read-modify-write no longer waits on them
 // in global memory (12 KB more shared memory: 5 CTAs per SM).
-template <int R, int TZ, bool ENERGY, bool PF = false>
+// QD (no energy terms): a.fwd is the difference set of S_{t+1} (planes
+// Q_*), written by the forward step, so the imaging reads five values per
+// cell instead of differencing the stored state.  (Without the difference
+// windows it fits 32 registers and 7 CTAs per SM, measured slower on B200
+// than 6: 0.96 against 0.83 ms per 64-shot launch.)
+template <int R, int TZ, bool ENERGY, bool PF = false, int QD = 0>
 __global__ void __launch_bounds__(NTHREADS, (R == 2 && !ENERGY) ? (PF ? 5 : 6) : 1)
     adj_step(const __grid_constant__ AdjArgs a)
 {
@@ -1495,7 +1637,7 @@ __global__ void __launch_bounds__(NTHREADS, (R == 2 && !ENERGY) ? (PF ? 5 : 6) :
     const int r0 = (tid / TX) * NK;
     const long long pz = g.pitch;
     float wvz[2 * R + 1], wtz[2 * R + 1], wtxz[2 * R + 1];
-    const bool win = F && gj >= glo && gj <= g.tnx - R - a.npml && i0 + r0 + NK - 1 >= glo &&
+    const bool win = QD == 0 && F && gj >= glo && gj <= g.tnx - R - a.npml && i0 + r0 + NK - 1 >= glo &&
                      i0 + r0 <= g.tnz - R - a.npml;
     if (win) {
         const long long c0 = cell_off(g, i0 + r0, gj);
@@ -1532,6 +1674,7 @@ __global__ void __launch_bounds__(NTHREADS, (R == 2 && !ENERGY) ? (PF ? 5 : 6) :
         const float atx = out[TXX * P + co], atz = out[TZZ * P + co], atxz = out[TXZ * P + co];
         float dzp_vx, dxm_vz, dxp_vx, dzm_vz, dzp_tz, dxm_tx, dxp_txz, dzm_txz;
         float vx = 0.f, vz = 0.f, tx = 0.f, tz = 0.f, txz = 0.f;
+        if constexpr (!QD) {
         if (F) {
             // DzpVx is formed from vz, as the reference does (elastic.cl:485)
             dzp_vx = wfwd<R>(wvz, a.k.cz);
@@ -1582,7 +1725,21 @@ __global__ void __launch_bounds__(NTHREADS, (R == 2 && !ENERGY) ? (PF ? 5 : 6) :
 #undef BFWD
 #undef BBWD
         }
+        }
         const float b = __ldg(a.mat + 2 * P + co);
+        if constexpr (QD) {
+            const unsigned char *F8 = QD == 2 ? a.fwd8 + slot * a.fwd_stride : nullptr;
+            const float q0 = qld<QD>(F, F16, F8, Q_DXP_VX * P + co), q1 = qld<QD>(F, F16, F8, Q_DZM_VZ * P + co),
+                        q2 = qld<QD>(F, F16, F8, Q_VZS * P + co), q3 = qld<QD>(F, F16, F8, Q_TXS * P + co),
+                        q4 = qld<QD>(F, F16, F8, Q_TZS * P + co);
+            float gmu = G[0 * P + co], glam = G[1 * P + co], grho = G[2 * P + co];
+            gmu += 2.f * dt * (atx * q0 + atz * q1) + dt * atxz * q2;
+            glam += dt * (atx + atz) * (q0 + q1);
+            grho += -(dt * (b * b)) * (avx * q3 + avz * q4);
+            G[0 * P + co] = gmu;
+            G[1 * P + co] = glam;
+            G[2 * P + co] = grho;
+        } else {
         float gmu = PF ? s_g[(0 * TZ + r) * TX + c] : G[0 * P + co];
         float glam = PF ? s_g[(1 * TZ + r) * TX + c] : G[1 * P + co];
         float grho = PF ? s_g[(2 * TZ + r) * TX + c] : G[2 * P + co];
@@ -1601,12 +1758,30 @@ __global__ void __launch_bounds__(NTHREADS, (R == 2 && !ENERGY) ? (PF ? 5 : 6) :
                                     vz * vz * (dzp_tz * dzp_tz + dxp_txz * dxp_txz));
         }
         }
+        }
         // the residual the next step injects (Adj_injSrc, elastic_surface.cl:48-71),
         // added to this step's output after the imaging has read it
         if (a.epi_row >= 0) inject_epilogue(a, a.epi_row, slot, gi, gj, co, avx, avz, out);
         out[VX * P + co] = avx;
         out[VZ * P + co] = avz;
     }
+}
+
+// The stress planes (Q_TXS, Q_TZS) of the difference set of state S: for
+// the last state of a forward run or a recomputed segment, which no later
+// forward step reads.  The imaging domain of every slot; one thread per
+// cell, grid (ceil(tnx / 256), tnz, slots).
+template <int R, int QD>
+__global__ void __launch_bounds__(256) qstress_kernel(Grid g, Coef k, const float *in, long long in_stride, void *q,
+                                                      unsigned char *q8, long long q_stride, int npml)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    const int glo = npml + R;
+    if (i < glo || i > g.tnz - R - npml || j < glo || j > g.tnx - R - npml) return;
+    const long long P = g.plane, co = cell_off(g, i, j), qo = blockIdx.z * q_stride + co;
+    const float *S = in + blockIdx.z * in_stride;
+    qst1<QD>(q, q8, qo + Q_TXS * P, gbwd<R>(S + TXX * P, co, 1, k.cx) + gbwd<R>(S + TXZ * P, co, g.pitch, k.cz));
+    qst1<QD>(q, q8, qo + Q_TZS * P, gfwd<R>(S + TZZ * P, co, g.pitch, k.cz) + gfwd<R>(S + TXZ * P, co, 1, k.cx));
 }
 
 // ---------------------------------------------------------------------------

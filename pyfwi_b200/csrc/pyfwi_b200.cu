@@ -104,6 +104,8 @@ struct pyfwi_plan {
     bool exact_adj = false;  // PYFWI_ADJOINT_EXACT
     bool persist = false;    // time loops as persistent kernels (options.persist, where the layout allows)
     bool overlap = false;    // recompute of segment m-1 on a second stream beside the adjoint of segment m
+    int qd = 0;              // the segment store holds the imaging's differences of each state (options.store_diffs):
+                             // 1 in FP32, 2 in 24 bits (FP24 snapshots); 0 the states
     cudaStream_t side = nullptr;          // that second stream (created on first use)
     std::vector<cudaEvent_t> ovev;        // its events: [2m] recompute of m done, [2m+1] adjoint of m done
     int fwd_cap = 0, adj_cap = 0;  // co-resident CTAs of the persistent kernels on this device
@@ -176,15 +178,21 @@ int launch_fwd(pyfwi_plan *p, const StepArgs &a, int nslots, cudaStream_t s, boo
 {
     dim3 grid((p->g.tnx + TX - 1) / TX, (p->g.tnz + TZ - 1) / TZ, nslots);
     if (!reverse) {
-        size_t sm = FwdShape<R, TZ>::FLOATS * sizeof(float);
+        size_t sm = FwdShape<R, TZ>::FLOATS * sizeof(float), sm_q = sm + 4 * sizeof(float);
         static bool attr = false;
         if (!attr) {
             CK(cudaFuncSetAttribute(fwd_step<R, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
             CK(cudaFuncSetAttribute(fwd_step24<R, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            CK(cudaFuncSetAttribute(fwd_step<R, TZ, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_q));
+            CK(cudaFuncSetAttribute(fwd_step<R, TZ, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_q));
             attr = true;
         }
         if (a.snap8)  // 24-bit snapshots written by their own instance (keeps the others' registers)
             fwd_step24<R, TZ><<<grid, NTHREADS, sm, s>>>(a);
+        else if (a.qout && a.qout8)  // difference sets, also by their own instances
+            fwd_step<R, TZ, 2><<<grid, NTHREADS, sm_q, s>>>(a);
+        else if (a.qout)
+            fwd_step<R, TZ, 1><<<grid, NTHREADS, sm_q, s>>>(a);
         else
             fwd_step<R, TZ><<<grid, NTHREADS, sm, s>>>(a);
     } else {
@@ -243,6 +251,23 @@ int launch_adj_t(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
     AdjArgs b = a;
     b.nslots = nslots;
     if constexpr (own && !E) {
+        if (p->qd) {  // difference sets in the segment store (FP32) or the snapshot store (24 bits)
+            static bool attr_q = false;
+            if (!attr_q) {
+                CK(cudaFuncSetAttribute(adj_step<R, TZ, E, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sm));
+                CK(cudaFuncSetAttribute(adj_step<R, TZ, E, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sm));
+                attr_q = true;
+            }
+            if (p->qd == 2)
+                adj_step<R, TZ, E, false, 2><<<grid, NTHREADS, sm, s>>>(b);
+            else
+                adj_step<R, TZ, E, false, 1><<<grid, NTHREADS, sm, s>>>(b);
+            p->launches++;
+            CKL();
+            return PYFWI_OK;
+        }
         if (pf) {
             adj_step<R, TZ, E, true><<<grid, NTHREADS, sm_pf, s>>>(b);
             p->launches++;
@@ -269,7 +294,7 @@ int launch_adj_ns(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
 template <int R, int TZ>
 int launch_adj(pyfwi_plan *p, const AdjArgs &a, int nslots, cudaStream_t s)
 {
-    if (a.fwd8) {  // 24-bit snapshots: the 16-row kernel, one shot per CTA (the plan picks no other)
+    if (a.fwd8 && !p->qd) {  // 24-bit snapshots: the 16-row kernel, one shot per CTA (the plan picks no other)
         if (TZ != 16 || p->ans != 1) return fail(PYFWI_E_INVALID, "snapshots are imaged by adjoint variant 0 only");
         return p->nacc == 6 ? launch_adj_t<R, 16, true, 1, true>(p, a, nslots, s)
                             : launch_adj_t<R, 16, false, 1, true>(p, a, nslots, s);
@@ -559,7 +584,10 @@ bool fp24_snaps(const pyfwi_plan *p) { return bf16_snaps(p) && p->opt.snapshot =
 // exact mode, per slot of the store: M restart states S_0, S_seg, ...
 // S_{(M-1)seg}, then (FP32 snapshots) the seg states of the segment being
 // imaged.  With BF16 snapshots the segment states live in the BF16 store and
-// the FP32 chain that produces them runs in the two work states.
+// the FP32 chain that produces them runs in the two work states; with
+// difference sets (p->qd) slot k of the segment holds the imaging's
+// differences of S_{t_lo+k+1} instead of the state, and the chain runs in the
+// work states as well.
 // With overlap the segment states take two buffers: segment m uses buffer
 // m % 2, so the recompute of segment m - 1 can fill one while the adjoint of
 // segment m reads the other.
@@ -568,7 +596,8 @@ long long store_stride(const pyfwi_plan *p)
     return (long long)(p->M + (bf16_snaps(p) ? 0 : p->seg * (p->overlap ? 2 : 1))) * p->state;
 }
 
-// Stored state k (S_{t_lo+k+1}) of segment m, FP32 snapshots.
+// Stored state k (S_{t_lo+k+1}) of segment m, FP32 snapshots (or its
+// difference set).
 Buf seg_state(pyfwi_plan *p, void *ws, int m, int k)
 {
     const int buf = p->overlap ? (m & 1) : 0;
@@ -583,7 +612,8 @@ Buf exact_state(pyfwi_plan *p, void *ws, int s)
     long long sstride = store_stride(p);
     if (s == 0) return {store, sstride};
     if (p->M > 1 && s % p->seg == 0 && s / p->seg <= p->M - 1) return {store + (long long)(s / p->seg) * p->state, sstride};
-    if (s > (p->M - 1) * p->seg && !bf16_snaps(p)) return seg_state(p, ws, p->M - 1, s - (p->M - 1) * p->seg - 1);
+    if (s > (p->M - 1) * p->seg && !bf16_snaps(p) && !p->qd)
+        return seg_state(p, ws, p->M - 1, s - (p->M - 1) * p->seg - 1);
     return {work + (long long)(s & 1) * p->state, 2 * p->state};
 }
 
@@ -615,6 +645,10 @@ StepArgs base_step(pyfwi_plan *p, void *ws)
     a.nr = p->geom.nr;
     a.ns = p->geom.ns;
     a.trace_plane = (long long)p->geom.nt_ext * p->geom.ns * p->geom.nr;
+    // the imaging domain (Grad, elastic.cl:470): difference sets cover it
+    a.qlo = p->geom.npml + p->R;
+    a.qhi_z = p->g.tnz - p->R - p->geom.npml;
+    a.qhi_x = p->g.tnx - p->R - p->geom.npml;
     return a;
 }
 
@@ -724,6 +758,63 @@ int persist_backward(pyfwi_plan *p, void *ws, AdjArgs &a, int n, cudaStream_t st
 }
 
 // One forward pass of a group (exact mode), optionally recording traces.
+Buf work_state(pyfwi_plan *p, void *ws, int w)
+{
+    return {at<float>(ws, p->o_work) + (long long)w * p->state, 2 * p->state};
+}
+
+// Difference sets (p->qd): forward step t of segment m (first step t_lo)
+// writes the velocity planes of S_{t+1} into slot t - t_lo and the stress
+// planes of its input S_t into slot t - t_lo - 1; the stress planes of S_{t_lo}
+// belong to the segment before, which computes them from its last state.
+void set_diffs(pyfwi_plan *p, void *ws, StepArgs &a, int m, int t, int t_lo)
+{
+    a.qout = a.qin = nullptr;
+    a.qout8 = a.qin8 = nullptr;
+    if (!p->qd || t < t_lo) return;
+    a.snap = nullptr;  // the difference sets take the snapshots' place
+    a.snap8 = nullptr;
+    if (p->qd == 2) {  // 24 bits: the BF16 and byte planes of the snapshot store
+        a.qout = snap_at(p, ws, t - t_lo);
+        a.qout8 = snap8_at(p, ws, t - t_lo);
+        a.qin = t > t_lo ? snap_at(p, ws, t - t_lo - 1) : nullptr;
+        a.qin8 = t > t_lo ? snap8_at(p, ws, t - t_lo - 1) : nullptr;
+        a.q_stride = (long long)p->seg * p->state;
+        return;
+    }
+    a.qout = seg_state(p, ws, m, t - t_lo).base;
+    a.qin = t > t_lo ? seg_state(p, ws, m, t - t_lo - 1).base : nullptr;
+    a.q_stride = store_stride(p);
+}
+
+// The stress planes of the last state S_{t_hi} of segment m (in a work
+// state after the segment's steps), into its last slot.
+int last_diffs(pyfwi_plan *p, void *ws, int m, int t_hi, int n, cudaStream_t st)
+{
+    const Buf s = work_state(p, ws, t_hi & 1);
+    const int t_lo = m * p->seg, k = t_hi - 1 - t_lo;
+    dim3 grid((p->g.tnx + 255) / 256, p->g.tnz, n);
+    const int npml = p->geom.npml;
+    if (p->qd == 2) {
+        void *q = snap_at(p, ws, k);
+        unsigned char *q8 = snap8_at(p, ws, k);
+        const long long qs = (long long)p->seg * p->state;
+        if (p->R == 4)
+            qstress_kernel<4, 2><<<grid, 256, 0, st>>>(p->g, p->k, s.base, s.stride, q, q8, qs, npml);
+        else
+            qstress_kernel<2, 2><<<grid, 256, 0, st>>>(p->g, p->k, s.base, s.stride, q, q8, qs, npml);
+    } else {
+        float *q = seg_state(p, ws, m, k).base;
+        if (p->R == 4)
+            qstress_kernel<4, 1><<<grid, 256, 0, st>>>(p->g, p->k, s.base, s.stride, q, nullptr, store_stride(p), npml);
+        else
+            qstress_kernel<2, 1><<<grid, 256, 0, st>>>(p->g, p->k, s.base, s.stride, q, nullptr, store_stride(p), npml);
+    }
+    p->launches++;
+    CKL();
+    return PYFWI_OK;
+}
+
 int exact_pass(pyfwi_plan *p, void *ws, int s0, int n, float *traces, cudaStream_t st)
 {
     Buf z = exact_state(p, ws, 0);
@@ -747,9 +838,11 @@ int exact_pass(pyfwi_plan *p, void *ws, int s0, int n, float *traces, cudaStream
         a.snap = bf16_snaps(p) && t >= last_lo ? snap_at(p, ws, t - last_lo) : nullptr;
         a.snap8 = a.snap ? snap8_at(p, ws, t - last_lo) : nullptr;
         a.snap_stride = (long long)p->seg * p->state;
+        set_diffs(p, ws, a, p->M - 1, t, last_lo);
         int rc = step_fwd(p, a, n, st, false, at<float>(ws, 0));
         if (rc) return rc;
     }
+    if (p->qd) return last_diffs(p, ws, p->M - 1, p->geom.nt, n, st);
     return PYFWI_OK;
 }
 
@@ -759,11 +852,6 @@ Buf chp_state(pyfwi_plan *p, void *ws, int s0, int k)
     float *store = at<float>(ws, p->o_store);
     long long stride = (long long)p->chp.size() * p->state;
     return {store + (long long)s0 * stride + (long long)k * p->state, stride};
-}
-
-Buf work_state(pyfwi_plan *p, void *ws, int w)
-{
-    return {at<float>(ws, p->o_work) + (long long)w * p->state, 2 * p->state};
 }
 
 int reverse_pass(pyfwi_plan *p, void *ws, int s0, int n, float *traces, cudaStream_t st)
@@ -864,6 +952,11 @@ int recompute_segment(pyfwi_plan *p, void *ws, int s0, int n, int m, cudaStream_
     Range range("pyfwi recompute segment");
     for (int t = t_lo; t < t_hi; ++t) {
         Buf in = t > t_lo ? seg_state(p, ws, m, t - t_lo - 1) : exact_state(p, ws, t), out = seg_state(p, ws, m, t - t_lo);
+        if (p->qd) {  // the states in the work states, their differences in the segment
+            if (t > t_lo) in = work_state(p, ws, t & 1);
+            out = work_state(p, ws, (t + 1) & 1);
+        }
+        set_diffs(p, ws, f, m, t, t_lo);
         f.in = in.base;
         f.in_stride = in.stride;
         f.out = out.base;
@@ -874,6 +967,7 @@ int recompute_segment(pyfwi_plan *p, void *ws, int s0, int n, int m, cudaStream_
         int rc = step_fwd(p, f, n, st, false, at<float>(ws, 0));
         if (rc) return rc;
     }
+    if (p->qd) return last_diffs(p, ws, m, t_hi, n, st);
     return PYFWI_OK;
 }
 
@@ -1119,7 +1213,10 @@ int gradient_enqueue(pyfwi_plan *p, void *ws, const float *const *residual, int3
             f.shot0 = s0;
             for (int m = p->M - 1; m >= 0; --m) {
                 int t_lo = m * p->seg, t_hi = std::min((m + 1) * p->seg, G.nt);
-                if (m < p->M - 1) {  // recompute segment m from its restart state
+                if (m < p->M - 1 && p->qd) {
+                    rc = recompute_segment(p, ws, s0, n, m, st);
+                    if (rc) return rc;
+                } else if (m < p->M - 1) {  // recompute segment m from its restart state
                     Range range("pyfwi recompute segment");
                     for (int t = t_lo; t < t_hi; ++t) {
                         Buf in = exact_state(p, ws, t), out;
@@ -1413,6 +1510,13 @@ int pyfwi_plan_create(const pyfwi_geometry *geom, const int32_t *srcx, const int
     // segments, the reference adjoint
     p->overlap = opt->overlap && opt->checkpoint == PYFWI_CKPT_EXACT && p->M > 1 && opt->snapshot == PYFWI_SNAP_FP32 &&
                  !p->exact_adj;
+    // difference sets in the segment store: exact checkpoints in FP32, the
+    // reference adjoint without energy terms, the plain tile kernels
+    const bool qd = opt->store_diffs && opt->checkpoint == PYFWI_CKPT_EXACT &&
+                    (opt->snapshot == PYFWI_SNAP_FP32 || opt->snapshot == PYFWI_SNAP_FP24) && !p->exact_adj &&
+                    p->nacc == 3 && !p->persist && !p->st_w && !p->ftma && !p->ast_w && p->ans == 1 && !p->apf &&
+                    G.npml + p->R >= 4;  // whole 4-column groups are written: the imaged columns end 3 short of tnx
+    p->qd = qd ? (opt->snapshot == PYFWI_SNAP_FP24 ? 2 : 1) : 0;
 
     const size_t pf = (size_t)p->g.plane * sizeof(float), sb = (size_t)p->state * sizeof(float);
     // regions holding planes start on a row of the workspace (a multiple of
@@ -1519,6 +1623,13 @@ int pyfwi_launch_count(const pyfwi_plan *p, int64_t *count)
 {
     if (!p || !count) return fail(PYFWI_E_INVALID, "NULL argument");
     *count = p->launches;
+    return PYFWI_OK;
+}
+
+int pyfwi_plan_flags(const pyfwi_plan *p, int32_t *flags)
+{
+    if (!p || !flags) return fail(PYFWI_E_INVALID, "NULL argument");
+    *flags = (p->persist ? 1 : 0) | (p->overlap ? 2 : 0) | (p->qd ? 4 : 0);
     return PYFWI_OK;
 }
 

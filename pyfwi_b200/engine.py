@@ -85,6 +85,26 @@ class Plan:
         N.check(self.lib.pyfwi_launch_count(self.handle, ctypes.byref(c)))
         return c.value
 
+    def _flags(self):
+        f = ctypes.c_int32()
+        N.check(self.lib.pyfwi_plan_flags(self.handle, ctypes.byref(f)))
+        return f.value
+
+    @property
+    def persist(self):
+        """True when the plan runs its time loops as persistent kernels."""
+        return bool(self._flags() & 1)
+
+    @property
+    def overlap(self):
+        """True when the plan recomputes beside the adjoint on a second stream."""
+        return bool(self._flags() & 2)
+
+    @property
+    def store_diffs(self):
+        """True when the checkpoint segments hold the imaging's differences."""
+        return bool(self._flags() & 4)
+
     def misfit_gradient(self, src_vals, observed, mean_stress, adjoint, param, traces=None):
         """pyfwi_misfit_gradient: observed / adjoint are lists of 5 device
         tensors [nt_ext, ns*nr] or None.  Returns (grad [3, nz, nx], misfit

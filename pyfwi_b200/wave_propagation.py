@@ -29,7 +29,12 @@ stores every step in FP32 and the tile kernels run: True, False (the
 default), or 'auto': on where a step carries at most 2 M cell-shots),
 ``overlap`` (exact checkpoints in FP32 with recompute segments: recompute
 segment m - 1 on a second CUDA stream while the adjoint of segment m runs,
-with two segment buffers),
+with two segment buffers), ``store`` ('differences', the default: in exact
+mode with FP32 snapshots, the reference adjoint without energy terms and the
+tile kernels 0..2, the forward steps that fill the checkpoint segments store
+the five differences of each state that the imaging reads, and the adjoint
+step reads them instead of differencing the state; 'states': store the
+states),
 ``snapshot`` ('fp32'; 'bf16': the forward states the imaging reads are
 stored in BF16 while the forward recurrence stays FP32, halving their memory
 and their reads at the cost of rounding the imaged fields to 8 mantissa bits;
@@ -63,6 +68,8 @@ DEFAULT_TILE, SMALL_TILE, SMALL_SURVEY_CELLS = 0, 1, 8_000_000
 # inpa['overlap'] when absent: recompute segment m - 1 on a second stream
 # beside the adjoint of segment m
 OVERLAP_DEFAULT = False
+# inpa['store'] when absent
+STORE_DEFAULT = "differences"
 
 
 def _slice_bounds(start, stop, n):
@@ -306,6 +313,7 @@ class WavePreparation:
             o.graph = int(self._graph_on(inpa.get("graph", "auto"), batch))
             o.persist = int(self._persist_on(inpa.get("persist", False), batch))
             o.overlap = int(bool(inpa.get("overlap", OVERLAP_DEFAULT)))
+            o.store_diffs = int(store == "differences")
             o.chunk = int(inpa.get("chunk", 0))
             if chp is not None:
                 o.nchp = int(chp.size)
@@ -317,6 +325,9 @@ class WavePreparation:
             raise ValueError("inpa['adjoint'] must be 'reference' or 'exact'")
         if self.adjoint == "exact" and mode != "exact":
             raise ValueError("inpa['adjoint'] = 'exact' needs checkpoint 'exact'")
+        store = inpa.get("store", STORE_DEFAULT)
+        if store not in ("differences", "states"):
+            raise ValueError("inpa['store'] must be 'differences' or 'states'")
         snap = inpa.get("snapshot", "fp32")
         if snap not in ("fp32", "bf16", "fp24") or (snap != "fp32" and mode != "exact"):
             raise ValueError("inpa['snapshot'] must be 'fp32', 'bf16' or 'fp24' (the last two with checkpoint "

@@ -51,6 +51,21 @@ def test_no_write_outside_the_domains_variants(extra):
     assert W.plan.frame_check() == 0
 
 
+@pytest.mark.parametrize("name,extra", [("tiny_s8", {"energy_balancing": False, "segment": 7}),
+                                        ("tiny_s8", {"energy_balancing": False, "tile": 2}),
+                                        ("c1", {"store": "states"}), ("tiny_dtscale", {"segment": 11, "overlap": True}),
+                                        ("tiny_dtscale", {"snapshot": "fp24", "segment": 11}),
+                                        ("tiny_s8", {"energy_balancing": False, "snapshot": "fp24", "segment": 9}),
+                                        ("tiny_dxr", {"segment": 9, "tile": 1, "graph": True})])
+def test_no_write_outside_the_domains_stored_differences(name, extra):
+    """Difference sets in the checkpoint segments (the default where they
+    apply; the 8th-order stencil without energy terms, recompute segments,
+    overlap, graph replay), and stored states where they would apply."""
+    W = _run(name, **extra)
+    assert W.plan.store_diffs == (extra.get("store", "differences") == "differences")
+    assert W.plan.frame_check() == 0
+
+
 @pytest.mark.parametrize("name", ["tiny_dxr", "tiny_dtscale"])
 @pytest.mark.parametrize("snapshot", ["fp32", "bf16"])
 def test_no_write_outside_the_domains_exact_adjoint(name, snapshot):

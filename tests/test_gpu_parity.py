@@ -147,19 +147,102 @@ def test_overlapped_recompute_gives_the_same_bits(name, seg, batch):
         assert rel_l2(v, g["grad_" + k]) < GRAD_TOL, k
 
 
+def _c1_tile_corner_sources():
+    """C1 with its four sources where the stencils of the cells next to them
+    cross the 64 x 16 tile boundaries (padded cells (31, 63), (32, 64),
+    (31, 65), (33, 62))."""
+    case = cases.c1()
+    dh = case["inpa"]["dh"]
+    case["src_loc"] = np.array([[43, 11], [44, 12], [45, 11], [42, 13]], np.float32) * dh
+    case["name"] = "c1_corners"
+    return case
+
+
+@pytest.mark.parametrize("name,seg,batch,extra", [
+    ("c1", 0, 0, {}), ("c1", 50, 0, {}), ("c1", 37, 1, {"overlap": True}), ("c1_corners", 0, 0, {}),
+    ("c1_corners", 64, 2, {}), ("tiny_dtscale", 11, 0, {}), ("tiny_both", 13, 0, {}), ("tiny_water", 0, 0, {}),
+    ("tiny_dxr", 9, 0, {}), ("tiny_crosswell", 10, 0, {"checkpoint": "exact"}),
+    ("tiny_s8", 7, 0, {"energy_balancing": False}), ("tiny_s8", 0, 0, {"energy_balancing": False, "tile": 1}),
+    ("c1", 0, 0, {"tile": 2})])
+def test_stored_differences_match_stored_states(name, seg, batch, extra):
+    """inpa['store'] = 'differences': the forward steps that fill the
+    checkpoint segments store the five differences of each state the imaging
+    reads (the stress ones of a state written by the step that reads it, with
+    the source of that step taken out), and the adjoint step reads them.  The
+    seismograms are those of storing states bit for bit, the gradients agree to
+    float32 rounding (the same operations in the same order), and where the
+    case has golden fixtures they stay within the gradient bar."""
+    import torch
+    case = _c1_tile_corner_sources() if name == "c1_corners" else cases.by_name(name)
+    W0 = product(case, segment=seg, shot_batch=batch, store="states", **extra)
+    d_obs = W0.forward_modeling(case["model_obs"])
+    d_est = W0.forward_modeling(case["model_est"])
+    res = l2_residual_np(d_est, d_obs)
+    res = {k: v for k, v in res.items() if np.any(v)}
+    out = []
+    for store in ("states", "differences"):
+        W = product(case, segment=seg, shot_batch=batch, store=store, **extra)
+        d = W.forward_modeling(case["model_est"])
+        out.append((d, W.gradient(res, parameterization=case["param"])))
+        torch.cuda.synchronize()
+        assert W.plan.store_diffs == (store == "differences"), store
+    for k in out[0][0]:
+        assert np.array_equal(out[0][0][k], out[1][0][k]), ("seismogram", k)
+    for k, v in out[1][1].items():
+        assert rel_l2(v, out[0][1][k]) < 1e-6, (k, rel_l2(v, out[0][1][k]))
+    if name in cases.__dict__ and case["chpr"] == 100 and not extra:
+        g = load_golden(name)
+        res = l2_residual_np(_golden_section(g, "d_est_"), _golden_section(g, "d_obs_"))
+        res = {k: v for k, v in res.items() if np.any(v)}
+        W = product(case, segment=seg, shot_batch=batch)
+        W.forward_modeling(case["model_est"])
+        for k, v in W.gradient(res, parameterization=case["param"]).items():
+            assert rel_l2(v, g["grad_" + k]) < GRAD_TOL, ("grad", k)
+
+
+@pytest.mark.parametrize("name,seg,batch,extra", [
+    ("c1", 0, 0, {}), ("c1", 50, 0, {}), ("c1_corners", 64, 2, {}), ("tiny_dtscale", 11, 0, {}),
+    ("tiny_s8", 7, 0, {"energy_balancing": False})])
+def test_24_bit_stored_differences(name, seg, batch, extra):
+    """inpa['snapshot'] = 'fp24' with stored differences: the difference sets
+    kept in 24 bits (a BF16 plane and a byte plane, three quarters of the FP32
+    store).  Each value is rounded once, after the differencing, so the
+    gradient stays within 1e-5 of the FP32 difference sets (rounding the
+    states before differencing costs far more: test_gpu_fp64_error)."""
+    import torch
+    case = _c1_tile_corner_sources() if name == "c1_corners" else cases.by_name(name)
+    W0 = product(case, segment=seg, shot_batch=batch, **extra)
+    d_obs = W0.forward_modeling(case["model_obs"])
+    d_est = W0.forward_modeling(case["model_est"])
+    res = l2_residual_np(d_est, d_obs)
+    res = {k: v for k, v in res.items() if np.any(v)}
+    out = []
+    for snapshot in ("fp32", "fp24"):
+        W = product(case, segment=seg, shot_batch=batch, snapshot=snapshot, **extra)
+        d = W.forward_modeling(case["model_est"])
+        out.append((d, W.gradient(res, parameterization=case["param"])))
+        torch.cuda.synchronize()
+        assert W.plan.store_diffs
+    for k in out[0][0]:
+        assert np.array_equal(out[0][0][k], out[1][0][k]), ("seismogram", k)
+    for k, v in out[1][1].items():
+        assert rel_l2(v, out[0][1][k]) < 1e-5, (k, rel_l2(v, out[0][1][k]))
+
+
 def test_tile_variants_agree():
     """Tile kernels of every height give identical bits (forward and
     gradient); streaming kernels (other FMA grouping) agree to float32
     rounding; the variants whose adjoint CTAs carry several shots run the
     forward of variant 0 (identical bits) and sum the shots' imaging in
     another order (float32 rounding); the TMA-staged tile kernels give the
-    tile kernels' bits."""
+    tile kernels' bits.  All with stored states (difference sets apply to
+    the tile kernels 0..2 only: test_stored_differences_match_stored_states)."""
     case = cases.tiny_dxr()
     g = load_golden("tiny_dxr")
     res = l2_residual_np(_golden_section(g, "d_est_"), _golden_section(g, "d_obs_"))
     base = None
     for tile in range(12):
-        W = product(case, tile=tile)
+        W = product(case, tile=tile, store="states")
         d = W.forward_modeling(case["model_est"])
         gr = W.gradient(res, parameterization=case["param"])
         if base is None:

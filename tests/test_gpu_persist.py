@@ -46,7 +46,7 @@ def _evaluate(case, shot_batch=0, **extra):
 def test_persistent_loops_give_the_step_kernels_bits(name, batch):
     case = cases.by_name(name)
     Wp, *out_p = _evaluate(case, persist=True, shot_batch=batch)
-    Ws, *out_s = _evaluate(case, persist=False, shot_batch=batch)
+    Ws, *out_s = _evaluate(case, persist=False, shot_batch=batch, store="states")  # the step kernels' states path
     assert Wp.plan.opts.persist == 1 and Ws.plan.opts.persist == 0
     energy = case["inpa"].get("energy_balancing", False)
     for q, (a, b) in enumerate(zip(out_p, out_s)):
@@ -64,7 +64,7 @@ def test_persistent_loops_on_the_200x400_survey():
     case = cases.c2_parity()
     g = load_golden("c2_parity")
     Wp, d_obs, d_est, raw, grad = _evaluate(case, persist=True)
-    _, d_obs_s, d_est_s, _, grad_s = _evaluate(case, persist=False)
+    _, d_obs_s, d_est_s, _, grad_s = _evaluate(case, persist=False, store="states")
     for k in d_est:
         assert np.array_equal(d_est[k], d_est_s[k]) and np.array_equal(d_obs[k], d_obs_s[k]), k
         if "d_est_" + k in g:

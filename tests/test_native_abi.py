@@ -34,7 +34,7 @@ def test_exports_every_declared_symbol(native):
 
 
 def test_abi_version(native):
-    assert native.lib().pyfwi_abi_version() == native.ABI_VERSION == 7
+    assert native.lib().pyfwi_abi_version() == native.ABI_VERSION == 8
 
 
 def _geom(native, nz=20, nx=24, npml=4, ns=2, nr=10, half=2):
