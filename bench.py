@@ -361,22 +361,33 @@ def run_ours(args, world, rank, local):
                 "avg_launch_ms": ms_k / max(n_l, 1), "alg_bytes_per_launch": alg / max(n_l, 1)}
 
     names = {0: "fwd_step", 1: "adj_step", 2: "rev_step"}
-    per_kernel = {names[k]: kernel_roof(k) for k in prof if prof[k][0] > 0}
+
+    def traffic_for(k):
+        """ncu DRAM bytes per cell-shot of the benchmark's launch shape (a
+        one-pass capture under profiles/), times the cell-shots of this run's
+        average launch of kernel kind k; None where no capture matches."""
+        tp = os.path.join(ROOT, "profiles", "traffic_%s_c3%s.json"
+                          % (names[k], "_differences" if store == "differences" else ""))
+        if not os.path.exists(tp) or args.config != "c3":
+            return None, None
+        with open(tp) as f:
+            tj = json.load(f)
+        if tj.get("store", "states") != store or tj.get("snapshot", "fp32") != W_snapshot:
+            return None, None
+        return (tj["dram_bytes_per_cell_shot"] * prof[k][2] / max(prof[k][0], 1),
+                {"ncu_capture": tj.get("capture"), "shots_per_launch": tj.get("shots_per_launch"),
+                 "scaled_to": "cell-shots of this run's average launch"})
+
+    per_kernel = {}
+    for k in prof:
+        if prof[k][0] > 0:
+            per_kernel[names[k]] = kernel_roof(k)
+            per_kernel[names[k]]["traffic"] = traffic_for(k)[0]
     # dominant kernel: the one with the most device time
     dom = max(prof, key=lambda k: prof[k][1])
     name = names[dom]
     kr = per_kernel[name]
-    traffic, traffic_src = None, None
-    tp = os.path.join(ROOT, "profiles", "traffic_%s_c3.json" % name)
-    if os.path.exists(tp) and args.config == "c3":
-        with open(tp) as f:
-            tj = json.load(f)
-        if tj.get("store", "states") == store and tj.get("snapshot", "fp32") == W_snapshot:
-            # ncu DRAM bytes per cell-shot of one launch of the profile's
-            # capture, times the cell-shots of this run's average launch
-            traffic = tj["dram_bytes_per_cell_shot"] * prof[dom][2] / max(prof[dom][0], 1)
-            traffic_src = {"ncu_capture": tj.get("capture"), "shots_per_launch": tj.get("shots_per_launch"),
-                           "scaled_to": "cell-shots of this run's average launch"}
+    traffic, traffic_src = traffic_for(dom)
     roof = {"bound": "hbm", "kernel": name, "achieved": kr["achieved"], "peak": hbm, "unit": "GB/s",
             "frac": kr["frac"], "traffic": traffic, "traffic_source": traffic_src, "peak_source": peak_src,
             "launches": kr["launches"], "avg_launch_ms": kr["avg_launch_ms"],
