@@ -433,7 +433,9 @@ class WavePreparation:
             while hi - lo > 1:
                 mid = (lo + hi) // 2
                 lo, hi = (mid, hi) if fits(mid, b) else (lo, mid)
-            return lo
+            # the same number of segments, evened out: fewer recomputed steps
+            # ((M - 1) * s) in a smaller store
+            return -(-nt // (-(-nt // lo)))
 
         def group_cost(s, b):
             m = -(-nt // s)

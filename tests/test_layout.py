@@ -56,6 +56,10 @@ def test_c3_keeps_all_shots_in_one_group(free_memory):
     # the store holds ceil(nt / seg) restart states + seg states of 64 shots
     state = 20.0 * int(W.tnz) * int(W.tnx) * 64
     assert (-(-int(W.nt) // seg) + seg) * state <= ws
+    # segments evened out: no shorter segment count would recompute fewer steps
+    nt = int(W.nt)
+    m = -(-nt // seg)
+    assert seg == -(-nt // m), (seg, m)
 
 
 def test_thrust_belt_survey_fits_and_fills_the_gpu(free_memory):
