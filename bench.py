@@ -408,7 +408,7 @@ def run_ours(args, world, rank, local):
     if world == 1 and args.inversion > 0:
         gc.collect()
         torch.cuda.empty_cache()
-        inversion = {opt: inversion_run(args, case, dev, opt) for opt in ("device", "scipy")}
+        inversion = {opt: inversion_run(args, case, dev, opt) for opt in args.optimizers.split(",")}
     cpu = None
     if world == 1 and not args.no_cpu:
         v, kind, cores, desc = cpu_sample(survey(1), seconds=args.cpu_seconds)
@@ -652,6 +652,8 @@ def main():
                     help="shots of the plain one-shot-per-launch form timed beside the batched one (0: skip)")
     ap.add_argument("--inversion", type=int, default=0,
                     help="also time this many L-BFGS iterations of FWI (device and host optimiser)")
+    ap.add_argument("--optimizers", default="device,scipy",
+                    help="with --inversion: the optimisers to time (device: FWI's L-BFGS on the GPU; scipy: on the host)")
     ap.add_argument("--uneven", type=int, default=0,
                     help="also time a batch of this many uneven-size surveys (sequential, streams, graph)")
     ap.add_argument("--config", choices=["c3", "c5"], default="c3",

@@ -827,6 +827,12 @@ __global__ void __launch_bounds__(NTHREADS, QD ? (R == 2 ? 4 : 2) : 0) fwd_step(
     const int tid = threadIdx.x;
     const float dt = a.k.dt;
 
+    // the source cell, read while the tile's copies are in flight
+    int src_i = 0, src_j = 0;
+    if (a.add_src && tid == 0) {
+        src_i = __ldg(a.srcz + shot);
+        src_j = __ldg(a.srcx + shot);
+    }
     // every copy of the tile in flight at once, then one wait
     for (int e = tid; e < HT * (SW / 4); e += NTHREADS) {
         int r = e / (SW / 4), q = e - r * (SW / 4);
@@ -849,8 +855,9 @@ __global__ void __launch_bounds__(NTHREADS, QD ? (R == 2 ? 4 : 2) : 0) fwd_step(
     }
     cp_wait_all();
     __syncthreads();
-    if (a.add_src && tid == 0) {  // wave_propagation.py:652-664, elastic_surface.cl:23-28
-        const int si = a.srcz[shot], sj = a.srcx[shot];
+    if (a.add_src) {  // wave_propagation.py:652-664, elastic_surface.cl:23-28 (uniform: a barrier only then)
+      if (tid == 0) {
+        const int si = src_i, sj = src_j;
         const int ct = sj - (j0 - 8), cv = sj - (j0 - 4), rt = si - (i0 - 2 * R), rv = si - (i0 - R);
         if (ct >= 0 && ct < SW && rt >= 0 && rt < HT) {
             if constexpr (QD) {  // the stored input state has no source of this step
@@ -864,8 +871,9 @@ __global__ void __launch_bounds__(NTHREADS, QD ? (R == 2 ? 4 : 2) : 0) fwd_step(
             s_vx[rv * VW + cv] += a.src.x;
             s_vz[rv * VW + cv] += a.src.y;
         }
+      }
+      __syncthreads();
     }
-    __syncthreads();
 
     // velocities (update_velx / update_velz) on rows i0-R .. and columns
     // j0-4 .., 4 columns per thread

@@ -652,6 +652,11 @@ StepArgs base_step(pyfwi_plan *p, void *ws)
     return a;
 }
 
+// A source sample whose four components are zero adds nothing (x + 0 = x,
+// up to the sign of a zero), so its step skips the add and the forward
+// kernel's barrier after it; the reference adds it (elastic_surface.cl:23-28).
+bool src_adds(const float4 &v) { return v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f; }
+
 float4 src_at(const pyfwi_plan *p, int inj)
 {
     if (inj < 0 || inj >= (int)(p->src_vals.size() / 4)) return make_float4(0.f, 0.f, 0.f, 0.f);
@@ -831,8 +836,8 @@ int exact_pass(pyfwi_plan *p, void *ws, int s0, int n, float *traces, cudaStream
         a.out_stride = out.stride;
         bool inj = t % p->geom.dt_scale == 0;
         int k = t / p->geom.dt_scale;
-        a.add_src = inj;
         a.src = src_at(p, k);
+        a.add_src = inj && src_adds(a.src);
         a.rec_row = (inj && traces && k < p->geom.nt_ext) ? k : -1;
         const int last_lo = (p->M - 1) * p->seg;
         a.snap = bf16_snaps(p) && t >= last_lo ? snap_at(p, ws, t - last_lo) : nullptr;
@@ -881,8 +886,8 @@ int reverse_pass(pyfwi_plan *p, void *ws, int s0, int n, float *traces, cudaStre
         a.out_stride = out.stride;
         bool inj = t % p->geom.dt_scale == 0;
         int k = t / p->geom.dt_scale;
-        a.add_src = inj;
         a.src = src_at(p, k);
+        a.add_src = inj && src_adds(a.src);
         a.rec_row = (inj && traces && k < p->geom.nt_ext) ? k : -1;
         int rc = step_fwd(p, a, n, st, false, at<float>(ws, 0));
         if (rc) return rc;
@@ -961,8 +966,8 @@ int recompute_segment(pyfwi_plan *p, void *ws, int s0, int n, int m, cudaStream_
         f.in_stride = in.stride;
         f.out = out.base;
         f.out_stride = out.stride;
-        f.add_src = t % G.dt_scale == 0;
         f.src = src_at(p, t / G.dt_scale);
+        f.add_src = t % G.dt_scale == 0 && src_adds(f.src);
         f.rec_row = -1;
         int rc = step_fwd(p, f, n, st, false, at<float>(ws, 0));
         if (rc) return rc;
@@ -1076,8 +1081,8 @@ int exact_backward(pyfwi_plan *p, void *ws, const float *const *residual, int s0
                 f.in_stride = in.stride;
                 f.out = out.base;
                 f.out_stride = out.stride;
-                f.add_src = t % G.dt_scale == 0;
                 f.src = src_at(p, t / G.dt_scale);
+                f.add_src = t % G.dt_scale == 0 && src_adds(f.src);
                 f.rec_row = -1;
                 rc = step_fwd(p, f, n, st, false, at<float>(ws, 0));
                 if (rc) return rc;
@@ -1235,8 +1240,8 @@ int gradient_enqueue(pyfwi_plan *p, void *ws, const float *const *residual, int3
                         f.out = out.base;
                         f.out_stride = out.stride;
                         bool inj = t % G.dt_scale == 0;
-                        f.add_src = inj;
                         f.src = src_at(p, t / G.dt_scale);
+                        f.add_src = inj && src_adds(f.src);
                         f.rec_row = -1;
                         rc = step_fwd(p, f, n, st, false, at<float>(ws, 0));
                         if (rc) return rc;
