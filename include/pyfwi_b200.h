@@ -34,6 +34,10 @@ extern "C" {
 
 #define PYFWI_ABI_VERSION 8
 
+/* The most kernel launches a call replays as one CUDA graph (options.graph);
+ * calls with more launch directly. */
+#define PYFWI_GRAPH_MAX_LAUNCHES 400000LL
+
 enum pyfwi_status {
     PYFWI_OK = 0,
     PYFWI_E_INVALID = -1,   /* bad argument or geometry */
@@ -125,7 +129,8 @@ typedef struct pyfwi_options {
                                tile staged by TMA box copies (adjoint as 0..2), 11 the
                                16-row tile kernels whose adjoint prefetches the tile's
                                gradient accumulators into shared memory */
-    int32_t graph;          /* 1: replay time loops as CUDA graphs */
+    int32_t graph;          /* 1: replay time loops as CUDA graphs (calls of more than
+                               PYFWI_GRAPH_MAX_LAUNCHES kernel launches run directly) */
     int32_t chunk;          /* streaming kernels: grid rows per CTA, 0 = from the grid size */
     int32_t adj_tile;       /* adjoint+imaging step variant + 1 (same numbering as tile); 0 = tile */
     int32_t adjoint;        /* enum pyfwi_adjoint */

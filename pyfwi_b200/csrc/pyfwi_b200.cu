@@ -1356,17 +1356,29 @@ int forward_enqueue(pyfwi_plan *p, void *ws, float *traces, cudaStream_t st)
     return PYFWI_OK;
 }
 
+// Kernel launches of one pyfwi_forward (backward false) or one gradient
+// call (backward true), from the layout: per shot group nt forward steps,
+// and for a gradient the recomputed steps, nt adjoint steps and a few more.
+long long call_launches(const pyfwi_plan *p, bool backward)
+{
+    const long long nt = p->geom.nt, per = backward ? 2 * nt + (long long)(p->M - 1) * p->seg + p->M + 16 : nt + 4;
+    return (long long)p->ngroups * per;
+}
+
 // Replay `enqueue` as a CUDA graph: captured once per distinct key (the
 // pointers and values the launches bake in) on the plan's own stream, then
 // launched on the caller's stream.  A caller stream that is being captured
-// already (the caller builds its own graph) gets the launches directly.
+// already (the caller builds its own graph) gets the launches directly, and
+// so does a call of more than PYFWI_GRAPH_MAX_LAUNCHES launches (a graph of
+// millions of nodes exhausts host memory while it is captured; its launches
+// are long enough that issuing them costs little).
 template <typename F>
 int run_graph(pyfwi_plan *p, pyfwi_plan::GraphCache &c, const std::vector<uintptr_t> &key, cudaStream_t st,
-              F enqueue)
+              long long launches, F enqueue)
 {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(st, &cs));
-    if (cs != cudaStreamCaptureStatusNone) return enqueue(st);
+    if (cs != cudaStreamCaptureStatusNone || launches > PYFWI_GRAPH_MAX_LAUNCHES) return enqueue(st);
     if (!c.exec || c.key != key) {
         if (c.exec) {
             cudaGraphExecDestroy(c.exec);
@@ -1785,7 +1797,7 @@ int pyfwi_forward(pyfwi_plan *p, void *ws, size_t bytes, const float *src_vals, 
         key.push_back(b);
     }
     rc = p->opt.graph && !p->profiling
-             ? run_graph(p, p->gfwd, key, st, [&](cudaStream_t s) { return forward_enqueue(p, ws, traces, s); })
+             ? run_graph(p, p->gfwd, key, st, call_launches(p, false), [&](cudaStream_t s) { return forward_enqueue(p, ws, traces, s); })
              : forward_enqueue(p, ws, traces, st);
     if (rc) return rc;
     p->fwd_valid = true;
@@ -1809,7 +1821,7 @@ int pyfwi_gradient(pyfwi_plan *p, void *ws, size_t bytes, const float *const *re
         key.push_back(b);
     }
     rc = p->opt.graph && !p->profiling
-             ? run_graph(p, p->ggrad, key, st,
+             ? run_graph(p, p->ggrad, key, st, call_launches(p, true),
                          [&](cudaStream_t s) { return gradient_enqueue(p, ws, residual, param, grad, raw, s); })
              : gradient_enqueue(p, ws, residual, param, grad, raw, st);
     if (rc) return rc;
@@ -1858,7 +1870,7 @@ int pyfwi_misfit_gradient(pyfwi_plan *p, void *ws, size_t bytes, const float *sr
         key.push_back(b);
     }
     rc = p->opt.graph && !p->profiling
-             ? run_graph(p, p->gmis, key, st,
+             ? run_graph(p, p->gmis, key, st, call_launches(p, true),
                          [&](cudaStream_t s) { return gradient_enqueue(p, ws, nullptr, param, grad, nullptr, s, &mf); })
              : gradient_enqueue(p, ws, nullptr, param, grad, nullptr, st, &mf);
     if (rc) return rc;

@@ -23,7 +23,8 @@ variant when it differs from ``tile``), ``chunk`` (rows per CTA of the
 streaming variants), ``graph`` (replay whole calls as CUDA graphs: True,
 False, or 'auto', the default: on where a launch carries at most 8 M
 cell-shots, where issuing launches from the host would cost a noticeable
-share), ``persist`` (run the time loops as persistent cooperative kernels,
+share, and a call issues at most GRAPH_MAX_LAUNCHES launches; the library
+runs longer calls directly either way), ``persist`` (run the time loops as persistent cooperative kernels,
 many steps per launch with a grid barrier between steps, where the layout
 stores every step in FP32 and the tile kernels run: True, False (the
 default), or 'auto': on where a step carries at most 2 M cell-shots),
@@ -310,7 +311,7 @@ class WavePreparation:
             o.energy = 1 if self.energy_balancing and self.adjoint != "exact" else 0
             o.tile, o.adj_tile = variants
             o.adjoint = N.ADJOINT_EXACT if self.adjoint == "exact" else N.ADJOINT_REFERENCE
-            o.graph = int(self._graph_on(inpa.get("graph", "auto"), batch))
+            o.graph = int(self._graph_on(inpa.get("graph", "auto"), batch, seg))
             o.persist = int(self._persist_on(inpa.get("persist", False), batch))
             o.overlap = int(bool(inpa.get("overlap", OVERLAP_DEFAULT)))
             o.store_diffs = int(store == "differences")
@@ -357,6 +358,9 @@ class WavePreparation:
     # 1.08x); above it the kernels hide the issue cost and the copies into
     # the captured buffers are pure overhead
     GRAPH_AUTO_CELLS = 8_000_000
+    # and where a gradient call issues at most this many launches (the
+    # library's PYFWI_GRAPH_MAX_LAUNCHES: it runs longer calls directly)
+    GRAPH_MAX_LAUNCHES = 400_000
 
     # 'auto' runs the time loops as persistent kernels (many steps per
     # cooperative launch, a grid barrier between steps) where a step carries
@@ -378,10 +382,13 @@ class WavePreparation:
             raise ValueError("inpa['persist'] must be True, False or 'auto'")
         return bool(persist)
 
-    def _graph_on(self, graph, batch):
+    def _graph_on(self, graph, batch, seg=0):
         if graph == "auto":
             b = int(batch) if batch else int(self.ns)
-            return int(self.tnz) * int(self.tnx) * b <= self.GRAPH_AUTO_CELLS
+            nt, s = int(self.nt), int(seg) if seg and int(seg) < int(self.nt) else int(self.nt)
+            m = -(-nt // s)
+            launches = -(-int(self.ns) // b) * (2 * nt + (m - 1) * s + m + 16)
+            return int(self.tnz) * int(self.tnx) * b <= self.GRAPH_AUTO_CELLS and launches <= self.GRAPH_MAX_LAUNCHES
         if graph not in (True, False, 0, 1):
             raise ValueError("inpa['graph'] must be True, False or 'auto'")
         return bool(graph)

@@ -86,3 +86,18 @@ def test_less_memory_gives_shorter_segments_or_smaller_groups(free_memory):
         out.append((seg, batch))
     (s1, b1), (s2, b2) = out
     assert s2 * b2 <= s1 * b1
+
+
+def test_graph_auto_stays_off_for_calls_of_many_launches(free_memory):
+    """'auto' graph replay: small launches (at most 8 M cell-shots) and calls
+    of at most GRAPH_MAX_LAUNCHES launches.  The thrust-belt survey in groups
+    of 2 shots (what the layout takes with the observed data of an inversion
+    resident) issues over a million launches per gradient: no graph.  The
+    100 x 100 survey, one group: graph."""
+    free_memory(155 * GB)
+    W, seg, batch, _ = _layout(cases.c5())
+    assert int(W.tnz) * int(W.tnx) * batch <= W.GRAPH_AUTO_CELLS
+    assert not W._graph_on("auto", batch, seg)
+    assert W._graph_on(True, batch, seg)  # an explicit request stands (the library runs it directly)
+    W1 = product(cases.c1(), cuda_device="cpu")
+    assert W1._graph_on("auto", 0, 0)
