@@ -36,7 +36,7 @@ extern "C" {
 
 /* The most kernel launches a call replays as one CUDA graph (options.graph);
  * calls with more launch directly. */
-#define PYFWI_GRAPH_MAX_LAUNCHES 400000LL
+#define PYFWI_GRAPH_MAX_LAUNCHES 600000LL
 
 enum pyfwi_status {
     PYFWI_OK = 0,

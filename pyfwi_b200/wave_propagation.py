@@ -360,7 +360,7 @@ class WavePreparation:
     GRAPH_AUTO_CELLS = 8_000_000
     # and where a gradient call issues at most this many launches (the
     # library's PYFWI_GRAPH_MAX_LAUNCHES: it runs longer calls directly)
-    GRAPH_MAX_LAUNCHES = 400_000
+    GRAPH_MAX_LAUNCHES = 600_000
 
     # 'auto' runs the time loops as persistent kernels (many steps per
     # cooperative launch, a grid barrier between steps) where a step carries
