@@ -334,9 +334,11 @@ int pyfwi_barrier_selftest(pyfwi_plan *plan, void *workspace, size_t bytes, int6
  *             out of the misfit
  *   grad      [3][nz][nx] as pyfwi_gradient;  misfit: device double, overwritten
  * Plans whose workspace + traces + residuals exceed the array are rejected
- * (PYFWI_E_WORKSPACE, message gives the bytes needed).  The first call on a
- * device looks up the array's device address; make it before any stream
- * capture.  That address is kept until the process exits: after a
+ * (PYFWI_E_WORKSPACE, message gives the bytes needed).  No call of this
+ * entry point may be captured in a CUDA graph: the array is shared, so every
+ * call rebuilds the plan's setup in it, including a copy of the source cells
+ * from host memory.  The first call on a device looks up the array's device
+ * address.  That address is kept until the process exits: after a
  * cudaDeviceReset of the device, do not call this entry point again in the
  * same process.  All calls on a device share the array (each call clears
  * what it needs); calls that overlap on the GPU race. */
