@@ -501,17 +501,6 @@ __device__ __forceinline__ void qst1(void *q, unsigned char *q8, long long o, fl
         write_snap1(static_cast<__nv_bfloat16 *>(q), q8, o, v);
 }
 
-// Four values of one row from cell co (column gj) on: one float4 store when
-// the four columns are inside the grid, else one store per column.
-__device__ __forceinline__ void st4row(float *plane, long long co, int gj, int tnx, float4 v)
-{
-    if (gj + 3 < tnx) {
-        *reinterpret_cast<float4 *>(plane + co) = v;
-    } else {
-        for (int k = 0; k < 4 && gj + k < tnx; ++k) plane[co + k] = f4(v, k);
-    }
-}
-
 // Three aligned float4 of a shared row around column c (c - 4 .. c + 7).
 __device__ __forceinline__ void row12(float (&v)[12], const float *row, int c)
 {
