@@ -341,6 +341,31 @@ void orc_adj_update_v(const orc_cfg *g, orc_state *A, const orc_model *M)
     }
 }
 
+/* Test builds with IMG_ROUND set (REAL = float only) round the imaging's
+ * five differences of the forward state to nearest even before use: 1 at
+ * BF16 (8 mantissa bits), 2 at 24 bits (15 mantissa bits), as a store of
+ * difference sets in those formats would.  IMG_ROUND 0 (the oracle) leaves
+ * the expressions as they are. */
+#ifndef IMG_ROUND
+#define IMG_ROUND 0
+#endif
+#if IMG_ROUND
+static inline float img_round(float x)
+{
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if (IMG_ROUND == 1) {
+        u += 0x7FFFu + ((u >> 16) & 1u);
+        u &= 0xFFFF0000u;
+    } else {
+        u += 0x7Fu + ((u >> 8) & 1u);
+        u &= 0xFFFFFF00u;
+    }
+    memcpy(&x, &u, 4);
+    return x;
+}
+#endif
+
 /* ---- zero-lag imaging (elastic.cl:470-526) ------------------------------
  * G[0]=Gmu G[1]=Glam G[2]=Grho, G[3..5] the matching energy accumulators.
  * DzpVx is formed from vz, as in the reference (elastic.cl:485). */
@@ -360,14 +385,31 @@ void orc_grad(const orc_cfg *g, const orc_state *S, const orc_state *A, const or
             REAL DxmPx = dbwd(S->taux, c, 1, g, g->dx);
             REAL DxpPxz = dfwd(S->tauxz, c, 1, g, g->dx);
             REAL DzmPxz = dbwd(S->tauxz, c, Nx, g, g->dz);
+#if IMG_ROUND
+            /* the five imaged values rounded as a store of difference sets
+             * would keep them (test builds only, see img_round) */
+            DxpVx = img_round(DxpVx);
+            DzmVz = img_round(DzmVz);
+            const REAL q_vz = img_round(DzpVx + DxmVz), q_tx = img_round(DxmPx + DzmPxz), q_tz = img_round(DzpPz + DxpPxz);
+#define Q_VZ q_vz
+#define Q_TX q_tx
+#define Q_TZ q_tz
+#else
+#define Q_VZ (DzpVx + DxmVz)
+#define Q_TX (DxmPx + DzmPxz)
+#define Q_TZ (DzpPz + DxpPxz)
+#endif
             REAL tx = S->taux[c], tz = S->tauz[c], txz = S->tauxz[c], vx = S->vx[c], vz = S->vz[c];
             REAL rb = M->rho_b[c];
-            G[0][c] += 2 * dt * (A->taux[c] * DxpVx + A->tauz[c] * DzmVz) + dt * A->tauxz[c] * (DzpVx + DxmVz);
+            G[0][c] += 2 * dt * (A->taux[c] * DxpVx + A->tauz[c] * DzmVz) + dt * A->tauxz[c] * Q_VZ;
             G[3][c] += 4 * dt * dt * (tx * tx * DxpVx * DxpVx + tz * tz * DzmVz * DzmVz) +
                        dt * dt * txz * txz * (DzpVx * DzpVx + DxmVz * DxmVz);
             G[1][c] += dt * (A->taux[c] + A->tauz[c]) * (DxpVx + DzmVz);
             G[4][c] += dt * dt * (tx * tx + tz * tz) * (DxpVx * DxpVx + DzmVz * DzmVz);
-            G[2][c] += -(dt * (rb * rb)) * (A->vx[c] * (DxmPx + DzmPxz) + A->vz[c] * (DzpPz + DxpPxz));
+            G[2][c] += -(dt * (rb * rb)) * (A->vx[c] * Q_TX + A->vz[c] * Q_TZ);
+#undef Q_VZ
+#undef Q_TX
+#undef Q_TZ
             G[5][c] += dt * dt * (vx * vx * (DxmPx * DxmPx + DzmPxz * DzmPxz) + vz * vz * (DzpPz * DzpPz + DxpPxz * DxpPxz));
         }
 }

@@ -57,10 +57,17 @@ def build():
     subprocess.check_call(["make", "-s", "-C", HERE], stdout=subprocess.DEVNULL)
 
 
-def lib(precision="fp32"):
-    """ctypes handle of liborc32.so / liborc64.so, building them if absent."""
+def lib(precision="fp32", img_round=None):
+    """ctypes handle of liborc32.so / liborc64.so, building them if absent;
+    img_round 'bf16' / 'fp24' (precision 'fp32' only): the build whose
+    imaging rounds its five differences of the forward state to that format."""
     name = {"fp32": "liborc32.so", "fp64": "liborc64.so"}[precision]
-    if precision not in _LIBS:
+    if img_round:
+        if precision != "fp32" or img_round not in ("bf16", "fp24"):
+            raise ValueError("img_round is 'bf16' or 'fp24' on the fp32 oracle")
+        name = "liborc32_img%s.so" % img_round
+    key = (precision, img_round or None)
+    if key not in _LIBS:
         path = os.path.join(BUILD, name)
         if not os.path.exists(path):
             build()
@@ -75,8 +82,8 @@ def lib(precision="fp32"):
         L.orc_step_forward.argtypes = [ctypes.POINTER(OrcCfg)] + [P] * 10 + [ctypes.c_int]
         L.orc_exact_gradient_shot.argtypes = [ctypes.POINTER(OrcCfg), P, P, P, P, P, _i32, _i32, P, _i32,
                                               ctypes.POINTER(P), P, P, P, P]
-        _LIBS[precision] = L
-    return _LIBS[precision]
+        _LIBS[key] = L
+    return _LIBS[key]
 
 
 def _ptr(a):
@@ -216,13 +223,17 @@ class OracleWavePropagator:
     """CPU oracle with the reference ``WavePropagator`` interface.
 
     ``precision='fp32'`` reproduces the reference's float32 semantics,
-    ``'fp64'`` runs every array in double (the FP64 oracle).
+    ``'fp64'`` runs every array in double (the FP64 oracle).  ``img_round``
+    ('bf16' or 'fp24', fp32 only) rounds the imaging's five differences of
+    the forward state to that format (what a store of difference sets in it
+    would give): a what-if for the error of such a store, not the reference.
     """
 
     def __init__(self, inpa, src, rec_loc, model_shape, components=0, n_well_rec=0, chpr=0,
-                 precision="fp32"):
+                 precision="fp32", img_round=None):
         keys = [*inpa]
         self.precision = precision
+        self.img_round = img_round
         self.real = np.float32 if precision == "fp32" else np.float64
         # wave_propagation.py:28-35
         self.dt_scale = np.ceil(inpa["dt"] / 0.0006)
@@ -342,7 +353,7 @@ class OracleWavePropagator:
     def forward_shot(self, s, store=False):
         """Seismogram planes (5, nt_ext, nr) of shot s; with store=True also
         the checkpoint states (nchp, 5, tnz, tnx)."""
-        L = lib(self.precision)
+        L = lib(self.precision, self.img_round)
         seis = np.zeros((5, self.nt_ext, self.nr), self.real)
         W = np.zeros((self.nchp, 5, self.tnz, self.tnx), self.real) if store else None
         rc = L.orc_forward_shot(ctypes.byref(self.cfg), *self._mats(), int(self.srcx[s]), int(self.srcz[s]),
@@ -366,7 +377,7 @@ class OracleWavePropagator:
     def raw_gradient(self, res):
         """Six (tnz, tnx) accumulators (Gmu, Glam, Grho, and the three energy
         terms) summed over shots, from a prepared 2-D residual dict."""
-        L = lib(self.precision)
+        L = lib(self.precision, self.img_round)
         n = (int(self.tnz), int(self.tnx))
         G = [np.zeros(n, self.real) for _ in range(6)]
         for s in range(self.ns):
@@ -415,7 +426,7 @@ class OracleWavePropagator:
         """dJ/d(lam, mu, b) on the padded grid, summed over shots, for a
         misfit J of the raw traces with dJ/dtrace = dtrace ({field:
         (nt_ext, nr, ns)}, missing fields zero), the damping held fixed."""
-        L = lib(self.precision)
+        L = lib(self.precision, self.img_round)
         self._materials(model0)
         n = (int(self.tnz), int(self.tnx))
         G = [np.zeros(n, self.real) for _ in range(3)]
