@@ -238,6 +238,65 @@ def max_over_ranks(ms, world, dev):
     return float(t.item())
 
 
+def roofline(prof, ms, ncell, nint, ns, nt, steps, store, snapshot, hbm, peak_src, traffic_dir):
+    """The roofline object of the JSON line from the profiled step kernels.
+
+    prof[k] = (launches, device ms, cell-shots) of kernel kind k (0 forward,
+    1 adjoint + imaging, 2 reverse) over the timed steps, ms the timed
+    region.  Algorithmic bytes per cell-shot: BYTES_FWD / BYTES_ADJ, plus per
+    imaged cell (nint per shot-step) 5 imaged values at their stored width
+    and 3 gradients read and written; with difference sets the forward steps
+    also write every shot-step's five values once.  traffic: the ncu DRAM
+    bytes per cell-shot of a one-pass capture of the benchmark's launch shape
+    (traffic_dir/traffic_<kernel>_c3[_differences].json, matching store and
+    snapshot format), times this run's average launch; None without one."""
+    # bytes per value of what the imaging reads: FP32 states or difference
+    # sets, 24-bit (BF16 + byte) or BF16 snapshots
+    vb = {"fp32": 4.0, "fp24": 3.0, "bf16": 2.0}[snapshot]
+    q_bytes = 5 * vb * nint * int(ns) * int(nt) * steps if store == "differences" else 0.0
+    names = {0: "fwd_step", 1: "adj_step", 2: "rev_step"}
+
+    def kernel_roof(k):
+        n_l, ms_k, cells_k = prof[k]
+        if k == 1:
+            alg = cells_k * BYTES_ADJ + (cells_k / ncell) * nint * (5 * vb + 24.0)
+        else:
+            alg = cells_k * BYTES_FWD + (q_bytes if k == 0 else 0.0)
+        ach = alg / (ms_k * 1e-3) / 1e9 if ms_k > 0 else None
+        return {"achieved": ach, "frac": ach / hbm if ach else None, "launches": n_l,
+                "avg_launch_ms": ms_k / max(n_l, 1), "alg_bytes_per_launch": alg / max(n_l, 1)}
+
+    def traffic_for(k):
+        if traffic_dir is None:
+            return None, None
+        tp = os.path.join(traffic_dir, "traffic_%s_c3%s.json"
+                          % (names[k], "_differences" if store == "differences" else ""))
+        if not os.path.exists(tp):
+            return None, None
+        with open(tp) as f:
+            tj = json.load(f)
+        if tj.get("store", "states") != store or tj.get("snapshot", "fp32") != snapshot:
+            return None, None
+        return (tj["dram_bytes_per_cell_shot"] * prof[k][2] / max(prof[k][0], 1),
+                {"ncu_capture": tj.get("capture"), "shots_per_launch": tj.get("shots_per_launch"),
+                 "scaled_to": "cell-shots of this run's average launch"})
+
+    per_kernel = {}
+    for k in prof:
+        if prof[k][0] > 0:
+            per_kernel[names[k]] = kernel_roof(k)
+            per_kernel[names[k]]["traffic"] = traffic_for(k)[0]
+    dom = max(prof, key=lambda k: prof[k][1])  # dominant kernel: the most device time
+    kr = per_kernel[names[dom]]
+    traffic, traffic_src = traffic_for(dom)
+    return {"bound": "hbm", "kernel": names[dom], "achieved": kr["achieved"], "peak": hbm, "unit": "GB/s",
+            "frac": kr["frac"], "traffic": traffic, "traffic_source": traffic_src, "peak_source": peak_src,
+            "launches": kr["launches"], "avg_launch_ms": kr["avg_launch_ms"],
+            "alg_bytes_per_launch": kr["alg_bytes_per_launch"],
+            "kernel_share": {names[k]: prof[k][1] / max(ms, 1e-9) for k in prof},
+            "per_kernel": per_kernel}
+
+
 def run_ours(args, world, rank, local):
     import torch
     import torch.distributed as dist
@@ -342,58 +401,9 @@ def run_ours(args, world, rank, local):
     if world == 1 and args.plain_shots > 0:
         plain = plain_form(args, dev, batched_shots_s)
     hbm, peak_src = peaks()
-    store = "differences" if W_store_diffs else "states"
-    # bytes per value of what the imaging reads: FP32 states or difference
-    # sets, 24-bit (BF16 + byte) or BF16 snapshots
-    vb = {"fp32": 4.0, "fp24": 3.0, "bf16": 2.0}[W_snapshot]
-    # difference sets: every shot-step's set written once, by the forward
-    # step that produces (or reads) that state, over the imaged cells
-    q_bytes = 5 * vb * nint * int(shape["ns"]) * int(shape["nt"]) * args.steps if store == "differences" else 0.0
-
-    def kernel_roof(k):
-        n_l, ms_k, cells_k = prof[k]
-        if k == 1:  # propagation + imaging (interior cells: 5 imaged values, 3 gradients read and written)
-            alg = cells_k * BYTES_ADJ + (cells_k / ncell) * nint * (5 * vb + 24.0)
-        else:
-            alg = cells_k * BYTES_FWD + (q_bytes if k == 0 else 0.0)
-        ach = alg / (ms_k * 1e-3) / 1e9 if ms_k > 0 else None
-        return {"achieved": ach, "frac": ach / hbm if ach else None, "launches": n_l,
-                "avg_launch_ms": ms_k / max(n_l, 1), "alg_bytes_per_launch": alg / max(n_l, 1)}
-
-    names = {0: "fwd_step", 1: "adj_step", 2: "rev_step"}
-
-    def traffic_for(k):
-        """ncu DRAM bytes per cell-shot of the benchmark's launch shape (a
-        one-pass capture under profiles/), times the cell-shots of this run's
-        average launch of kernel kind k; None where no capture matches."""
-        tp = os.path.join(ROOT, "profiles", "traffic_%s_c3%s.json"
-                          % (names[k], "_differences" if store == "differences" else ""))
-        if not os.path.exists(tp) or args.config != "c3":
-            return None, None
-        with open(tp) as f:
-            tj = json.load(f)
-        if tj.get("store", "states") != store or tj.get("snapshot", "fp32") != W_snapshot:
-            return None, None
-        return (tj["dram_bytes_per_cell_shot"] * prof[k][2] / max(prof[k][0], 1),
-                {"ncu_capture": tj.get("capture"), "shots_per_launch": tj.get("shots_per_launch"),
-                 "scaled_to": "cell-shots of this run's average launch"})
-
-    per_kernel = {}
-    for k in prof:
-        if prof[k][0] > 0:
-            per_kernel[names[k]] = kernel_roof(k)
-            per_kernel[names[k]]["traffic"] = traffic_for(k)[0]
-    # dominant kernel: the one with the most device time
-    dom = max(prof, key=lambda k: prof[k][1])
-    name = names[dom]
-    kr = per_kernel[name]
-    traffic, traffic_src = traffic_for(dom)
-    roof = {"bound": "hbm", "kernel": name, "achieved": kr["achieved"], "peak": hbm, "unit": "GB/s",
-            "frac": kr["frac"], "traffic": traffic, "traffic_source": traffic_src, "peak_source": peak_src,
-            "launches": kr["launches"], "avg_launch_ms": kr["avg_launch_ms"],
-            "alg_bytes_per_launch": kr["alg_bytes_per_launch"],
-            "kernel_share": {names[k]: prof[k][1] / max(ms, 1e-9) for k in prof},
-            "per_kernel": per_kernel}
+    roof = roofline(prof, ms, ncell, nint, shape["ns"], shape["nt"], args.steps,
+                    "differences" if W_store_diffs else "states", W_snapshot, hbm, peak_src,
+                    os.path.join(ROOT, "profiles") if args.config == "c3" else None)
     small = None
     if world == 1 and args.configs:
         gc.collect()
