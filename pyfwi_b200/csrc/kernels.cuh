@@ -845,23 +845,23 @@ __global__ void __launch_bounds__(NTHREADS, QD ? (R == 2 ? 4 : 2) : 0) fwd_step(
     cp_wait_all();
     __syncthreads();
     if (a.add_src) {  // wave_propagation.py:652-664, elastic_surface.cl:23-28 (uniform: a barrier only then)
-      if (tid == 0) {
-        const int si = src_i, sj = src_j;
-        const int ct = sj - (j0 - 8), cv = sj - (j0 - 4), rt = si - (i0 - 2 * R), rv = si - (i0 - R);
-        if (ct >= 0 && ct < SW && rt >= 0 && rt < HT) {
-            if constexpr (QD) {  // the stored input state has no source of this step
-                s_mu[TZ * TX] = s_txx[rt * SW + ct];
-                s_mu[TZ * TX + 1] = s_tzz[rt * SW + ct];
+        if (tid == 0) {
+            const int si = src_i, sj = src_j;
+            const int ct = sj - (j0 - 8), cv = sj - (j0 - 4), rt = si - (i0 - 2 * R), rv = si - (i0 - R);
+            if (ct >= 0 && ct < SW && rt >= 0 && rt < HT) {
+                if constexpr (QD) {  // the stored input state has no source of this step
+                    s_mu[TZ * TX] = s_txx[rt * SW + ct];
+                    s_mu[TZ * TX + 1] = s_tzz[rt * SW + ct];
+                }
+                s_txx[rt * SW + ct] += a.src.z;
+                s_tzz[rt * SW + ct] += a.src.w;
             }
-            s_txx[rt * SW + ct] += a.src.z;
-            s_tzz[rt * SW + ct] += a.src.w;
+            if (cv >= 0 && cv < VW && rv >= 0 && rv < HV) {
+                s_vx[rv * VW + cv] += a.src.x;
+                s_vz[rv * VW + cv] += a.src.y;
+            }
         }
-        if (cv >= 0 && cv < VW && rv >= 0 && rv < HV) {
-            s_vx[rv * VW + cv] += a.src.x;
-            s_vz[rv * VW + cv] += a.src.y;
-        }
-      }
-      __syncthreads();
+        __syncthreads();
     }
 
     // velocities (update_velx / update_velz) on rows i0-R .. and columns
